@@ -1,0 +1,120 @@
+/* C ABI of the B200 KGraph library (libkgraph_b200.so).
+ *
+ * Plain pointers and sizes only.  Every call returns 0 on success and a
+ * non-zero KG_E_* code on failure; kg_last_error(ctx) then holds the message.
+ * The C++ API (kgraph.h) and the Python module are thin layers over these
+ * entry points, and a foreign binding (ctypes, cgo, JNI ...) can call them
+ * directly.  Each entry point names the reference interface it replaces.
+ *
+ * Pointers to rows, queries and outputs may be host or device (CUDA)
+ * memory; the library detects which and copies host buffers through pinned
+ * staging on the context's stream.  A context is bound to one GPU; calls on
+ * one context are serialised by an internal lock, so concurrent callers (the
+ * reference calls KGraph::search from many OpenMP threads,
+ * python-api.cpp:292-301) are safe.
+ */
+#ifndef KGRAPH_B200_H
+#define KGRAPH_B200_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct kg_ctx kg_ctx;
+
+enum { KG_METRIC_EUCLIDEAN = 0, KG_METRIC_ANGULAR = 1, KG_METRIC_L2SQR = 2 };
+enum {
+    KG_OK = 0,
+    KG_E_INVALID = 1,   /* kgraph::invalid_argument */
+    KG_E_RUNTIME = 2,   /* kgraph::runtime_error / std::runtime_error */
+    KG_E_IO = 3,        /* kgraph::io_error */
+    KG_E_CUDA = 4,      /* CUDA failure (allocation, launch) */
+    KG_E_DEVICE = 5     /* a kernel reported an error (lock spin limit, bad id) */
+};
+
+/* KGraph::IndexParams, kgraph.h:94-110 (same fields, same defaults). */
+typedef struct {
+    unsigned iterations, L, K, S, R, controls, seed;
+    float delta, recall;
+    unsigned prune;
+    int reverse;
+} kg_index_params;
+
+/* KGraph::IndexInfo, kgraph.h:135-147. stop_condition: 0 ITERATION, 1 DELTA, 2 RECALL. */
+typedef struct {
+    int stop_condition;
+    unsigned iterations;
+    float cost, recall, accuracy, delta, M;
+} kg_index_info;
+
+/* KGraph::SearchParams, kgraph.h:113-126. */
+typedef struct {
+    unsigned K, M, P, S, T;
+    float epsilon;
+    unsigned seed, init;
+} kg_search_params;
+
+/* Fills the reference's defaults (kgraph.h:14-37, 108, 124). */
+void kg_index_params_default(kg_index_params *p);
+void kg_search_params_default(kg_search_params *p);
+
+/* Creates a context on CUDA device `device` (KGraph::create, kgraph.h:199). */
+int kg_ctx_create(int device, kg_ctx **out);
+void kg_ctx_destroy(kg_ctx *ctx);
+const char *kg_last_error(kg_ctx *ctx);
+/* KGraph::version, kgraph.h:201. */
+const char *kg_version(void);
+/* kgraph::verbosity (kgraph.h:42): > 0 prints the per-iteration build log
+ * line of kgraph.cpp:952-962 to stderr. */
+void kg_set_verbosity(unsigned v);
+
+/* Binds the dataset: n rows of d floats, `stride_bytes` apart, copied into
+ * HBM with 64-byte aligned, zero-padded rows.  metric is KG_METRIC_*:
+ *   EUCLIDEAN  the Python oracle, half squared L2 (python-api.cpp:51-59)
+ *   ANGULAR    the Python oracle, -cos          (python-api.cpp:61-69)
+ *   L2SQR      MatrixOracle<.., metric::l2sqr>   (kgraph-data.h:38-61, 302-331)
+ * Replaces the dataset the reference's oracle wraps (NDArrayOracle ctor,
+ * python-api.cpp:110-114; MatrixProxy, kgraph-data.h:221-231). */
+int kg_set_data(kg_ctx *ctx, const float *rows, size_t n, size_t d, size_t stride_bytes, int metric);
+
+/* KGraph::build (kgraph.h:168; KGraphConstructor, kgraph.cpp:886-999).
+ * info may be NULL. */
+int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_info *info);
+
+/* Graph size for export: n nodes, E edges. */
+int kg_graph_size(kg_ctx *ctx, size_t *n, size_t *E);
+/* Copies the graph out as CSR: offsets[n+1], ids[E], dists[E] (may be NULL),
+ * M[n].  Backs KGraph::save / get_nn (kgraph.cpp:333-373, 566-582). */
+int kg_graph_export(kg_ctx *ctx, uint64_t *offsets, uint32_t *ids, float *dists, uint32_t *M);
+/* Installs a CSR graph (KGraph::load, kgraph.cpp:291-331).  dists may be NULL
+ * (FORMAT_NO_DIST); no_dist then marks distances unavailable. */
+int kg_graph_import(kg_ctx *ctx, size_t n, const uint64_t *offsets, const uint32_t *ids, const float *dists,
+                    const uint32_t *M);
+
+/* Batched KGraph::search (kgraph.h:197; KGraphImpl::search, kgraph.cpp:423-564)
+ * for nq queries of d floats, `q_stride_bytes` apart, in one launch.
+ * K_per_q / P_per_q (may be NULL) override params->K / params->P per query.
+ * Outputs are rows of out_ld entries (out_ld >= every K): ids[nq*out_ld],
+ * dists (may be NULL), counts[nq] (results returned, <= K), costs (may be
+ * NULL; SearchInfo.cost).  When params->init > 0, ids is also the input of the
+ * starting points (doc/params.md "User-Provided Starting Points").
+ * Without a graph every query takes the brute-force path
+ * (SearchOracle::search, kgraph.cpp:231-252; python-api.cpp:303-314). */
+int kg_search_batch(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes,
+                    const kg_search_params *params, const uint32_t *K_per_q, const uint32_t *P_per_q,
+                    size_t out_ld, uint32_t *ids, float *dists, uint32_t *counts, float *costs);
+
+/* KGraphImpl::reverse (kgraph.cpp:667-702) on the current graph. */
+int kg_reverse(kg_ctx *ctx, int rev_k);
+/* KGraph::prune (kgraph.h:180; kgraph.cpp:584-665) on the current graph. */
+int kg_prune(kg_ctx *ctx, unsigned level);
+
+/* Milliseconds of the last kg_build / kg_search_batch device work, measured
+ * with CUDA events on the context's stream (for profiling and benchmarks). */
+int kg_last_timing(kg_ctx *ctx, float *build_ms, float *search_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

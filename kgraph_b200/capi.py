@@ -1,0 +1,194 @@
+"""ctypes binding of the C-ABI (include/kgraph_b200.h).
+
+This is the binding a foreign caller would write; the tests and bench.py use
+it to drive the library exactly through its C entry points.  Loading fails
+loudly when the library has not been built: there is no fallback.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libkgraph_b200.so")
+
+METRIC = {"euclidean": 0, "angular": 1, "l2sqr": 2}
+
+# Every entry point include/kgraph_b200.h declares.
+SYMBOLS = [
+    "kg_index_params_default", "kg_search_params_default", "kg_ctx_create", "kg_ctx_destroy",
+    "kg_last_error", "kg_version", "kg_set_verbosity", "kg_set_data", "kg_build", "kg_graph_size",
+    "kg_graph_export", "kg_graph_import", "kg_search_batch", "kg_reverse", "kg_prune", "kg_last_timing",
+]
+
+
+class IndexParams(C.Structure):
+    _fields_ = [("iterations", C.c_uint), ("L", C.c_uint), ("K", C.c_uint), ("S", C.c_uint), ("R", C.c_uint),
+                ("controls", C.c_uint), ("seed", C.c_uint), ("delta", C.c_float), ("recall", C.c_float),
+                ("prune", C.c_uint), ("reverse", C.c_int)]
+
+
+class IndexInfo(C.Structure):
+    _fields_ = [("stop_condition", C.c_int), ("iterations", C.c_uint), ("cost", C.c_float), ("recall", C.c_float),
+                ("accuracy", C.c_float), ("delta", C.c_float), ("M", C.c_float)]
+
+
+class SearchParams(C.Structure):
+    _fields_ = [("K", C.c_uint), ("M", C.c_uint), ("P", C.c_uint), ("S", C.c_uint), ("T", C.c_uint),
+                ("epsilon", C.c_float), ("seed", C.c_uint), ("init", C.c_uint)]
+
+
+_lib = None
+
+
+def lib():
+    """Loads libkgraph_b200.so (raises if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libkgraph_b200.so is not built; run python -m kgraph_b200.build")
+        L = C.CDLL(LIB_PATH)
+        vp, sz = C.c_void_p, C.c_size_t
+        L.kg_ctx_create.argtypes = [C.c_int, C.POINTER(vp)]
+        L.kg_ctx_destroy.argtypes = [vp]
+        L.kg_last_error.argtypes = [vp]
+        L.kg_last_error.restype = C.c_char_p
+        L.kg_version.restype = C.c_char_p
+        L.kg_set_verbosity.argtypes = [C.c_uint]
+        L.kg_set_data.argtypes = [vp, vp, sz, sz, sz, C.c_int]
+        L.kg_build.argtypes = [vp, C.POINTER(IndexParams), C.POINTER(IndexInfo)]
+        L.kg_graph_size.argtypes = [vp, C.POINTER(sz), C.POINTER(sz)]
+        L.kg_graph_export.argtypes = [vp, vp, vp, vp, vp]
+        L.kg_graph_import.argtypes = [vp, sz, vp, vp, vp, vp]
+        L.kg_search_batch.argtypes = [vp, vp, sz, sz, C.POINTER(SearchParams), vp, vp, sz, vp, vp, vp, vp]
+        L.kg_reverse.argtypes = [vp, C.c_int]
+        L.kg_prune.argtypes = [vp, C.c_uint]
+        L.kg_last_timing.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.kg_index_params_default.argtypes = [C.POINTER(IndexParams)]
+        L.kg_search_params_default.argtypes = [C.POINTER(SearchParams)]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):   # torch tensor (device-resident buffers)
+        return C.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class KGError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+class Context:
+    """One kg_ctx: a dataset, a graph and a stream on one GPU."""
+
+    def __init__(self, device=0):
+        self.L = lib()
+        h = C.c_void_p()
+        r = self.L.kg_ctx_create(device, C.byref(h))
+        if r != 0:
+            raise KGError(r, "kg_ctx_create failed (no CUDA device?)")
+        self.h = h
+        self._keep = []
+
+    def close(self):
+        if self.h:
+            self.L.kg_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, r):
+        if r != 0:
+            raise KGError(r, self.L.kg_last_error(self.h).decode())
+
+    def set_data(self, X, metric="euclidean"):
+        m = METRIC[metric] if isinstance(metric, str) else int(metric)
+        if hasattr(X, "data_ptr"):
+            n, d = X.shape
+            stride = X.stride(0) * X.element_size()
+        else:
+            X = np.ascontiguousarray(X, np.float32)
+            n, d = X.shape
+            stride = X.strides[0]
+        self._check(self.L.kg_set_data(self.h, _ptr(X), n, d, stride, m))
+        self.n, self.d = n, d
+
+    def build(self, **kw):
+        p = IndexParams()
+        self.L.kg_index_params_default(C.byref(p))
+        for k, v in kw.items():
+            setattr(p, k, v)
+        info = IndexInfo()
+        self._check(self.L.kg_build(self.h, C.byref(p), C.byref(info)))
+        return {f: getattr(info, f) for f, _ in IndexInfo._fields_}
+
+    def graph(self):
+        n, E = C.c_size_t(), C.c_size_t()
+        self._check(self.L.kg_graph_size(self.h, C.byref(n), C.byref(E)))
+        off = np.zeros(n.value + 1, np.uint64)
+        ids = np.zeros(max(E.value, 1), np.uint32)
+        dists = np.zeros(max(E.value, 1), np.float32)
+        M = np.zeros(n.value, np.uint32)
+        self._check(self.L.kg_graph_export(self.h, _ptr(off), _ptr(ids), _ptr(dists), _ptr(M)))
+        return off, ids[: E.value], dists[: E.value], M
+
+    def set_graph(self, offsets, ids, dists, M):
+        offsets = np.ascontiguousarray(offsets, np.uint64)
+        ids = np.ascontiguousarray(ids, np.uint32)
+        M = np.ascontiguousarray(M, np.uint32)
+        dists = None if dists is None else np.ascontiguousarray(dists, np.float32)
+        self._check(self.L.kg_graph_import(self.h, len(M), _ptr(offsets), _ptr(ids), _ptr(dists), _ptr(M)))
+
+    def search(self, Q, K=25, P=100, M=0, S=10, T=1, epsilon=1e30, seed=1998, init=0, init_ids=None,
+               K_per_q=None, P_per_q=None, out_ld=None, with_cost=True):
+        """Returns (ids, dists, counts, costs) as numpy arrays (host path)."""
+        Q = np.ascontiguousarray(Q, np.float32)
+        nq = Q.shape[0]
+        p = SearchParams(K, M, P, S, T, epsilon, seed, init)
+        kmax = int(np.max(K_per_q)) if K_per_q is not None else K
+        ld = out_ld or max(kmax, 1)
+        ids = np.zeros((nq, ld), np.uint32)
+        if init_ids is not None:
+            ids[:, :init] = np.asarray(init_ids)[:, :init]
+        dists = np.zeros((nq, ld), np.float32)
+        counts = np.zeros(nq, np.uint32)
+        costs = np.zeros(nq, np.float32) if with_cost else None
+        kq = None if K_per_q is None else np.ascontiguousarray(K_per_q, np.uint32)
+        pq = None if P_per_q is None else np.ascontiguousarray(P_per_q, np.uint32)
+        self._check(self.L.kg_search_batch(self.h, _ptr(Q), nq, Q.strides[0], C.byref(p), _ptr(kq), _ptr(pq), ld,
+                                           _ptr(ids), _ptr(dists), _ptr(counts), _ptr(costs)))
+        return ids, dists, counts, costs
+
+    def search_raw(self, q_ptr, nq, q_stride, params, kq_ptr, pq_ptr, out_ld, ids_ptr, d_ptr, c_ptr, cost_ptr):
+        """kg_search_batch on raw (device or host) pointers."""
+        self._check(self.L.kg_search_batch(self.h, q_ptr, nq, q_stride, C.byref(params), kq_ptr, pq_ptr, out_ld,
+                                           ids_ptr, d_ptr, c_ptr, cost_ptr))
+
+    def reverse(self, k):
+        self._check(self.L.kg_reverse(self.h, k))
+
+    def prune(self, level):
+        self._check(self.L.kg_prune(self.h, level))
+
+    def timing(self):
+        b, s = C.c_float(), C.c_float()
+        self._check(self.L.kg_last_timing(self.h, C.byref(b), C.byref(s)))
+        return b.value, s.value
+
+
+def version():
+    return lib().kg_version().decode()
+
+
+def set_verbosity(v):
+    lib().kg_set_verbosity(v)

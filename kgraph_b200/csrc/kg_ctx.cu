@@ -1,0 +1,399 @@
+// C-ABI entry points: context, dataset, graph import/export, batched search.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <ctime>
+#include <map>
+#include <random>
+#include "kg_ctx.h"
+#include "kg_search.h"
+#include "kg_warp.cuh"
+
+using namespace kgb;
+
+namespace kgb {
+
+int set_error(kg_ctx *ctx, int code, const std::string &msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+int cuda_fail(kg_ctx *ctx, cudaError_t e, const char *what) {
+    return set_error(ctx, KG_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+bool is_device_ptr(const void *p) {
+    if (!p) return false;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+int check_device_error(kg_ctx *ctx, const char *what) {
+    uint32_t w = 0;
+    cudaError_t e = cudaMemcpyAsync(&w, ctx->errw.p, sizeof(w), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, what);
+    if (!w) return KG_OK;
+    cudaMemsetAsync(ctx->errw.p, 0, sizeof(uint32_t), ctx->stream);
+    std::string m = std::string(what) + ": device reported";
+    if (w & ERR_LOCK_TIMEOUT) m += " lock-spin limit reached;";
+    if (w & ERR_CAPACITY) m += " list capacity exceeded;";
+    if (w & ERR_BAD_ID) m += " node id out of range;";
+    if (w & ERR_INIT_K) { return set_error(ctx, KG_E_INVALID, "L < params.K"); }
+    return set_error(ctx, KG_E_DEVICE, m);
+}
+
+// GenRandom (kgraph.cpp:44-65): `size` distinct ids below N.
+void gen_random(std::mt19937 &rng, uint32_t *addr, uint32_t size, uint32_t N) {
+    if (N == size) {
+        for (uint32_t i = 0; i < size; ++i) addr[i] = i;
+        return;
+    }
+    for (uint32_t i = 0; i < size; ++i) addr[i] = rng() % (N - size);
+    std::sort(addr, addr + size);
+    for (uint32_t i = 1; i < size; ++i)
+        if (addr[i] <= addr[i - 1]) addr[i] = addr[i - 1] + 1;
+    uint32_t off = rng() % N;
+    for (uint32_t i = 0; i < size; ++i) addr[i] = (addr[i] + off) % N;
+}
+
+}  // namespace kgb
+
+namespace {
+
+// Per-row norm term of the metric (NDArrayOracle ctor, python-api.cpp:110-114),
+// one 4-lane group per row.
+__global__ void norms_kernel(DataView D, float *norms) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t gid = (blockIdx.x * blockDim.x + threadIdx.x) >> 2;
+    const uint32_t ngroups = (gridDim.x * blockDim.x) >> 2;
+    const uint32_t rounds = (D.n + ngroups - 1) / ngroups;
+    for (uint32_t r = 0; r < rounds; ++r) {
+        uint32_t row = gid + r * ngroups;
+        uint32_t safe = row < D.n ? row : 0;
+        const float *x = D.X + (size_t)safe * D.ld;
+        float n2 = group4_raw(x, x, D.d, METRIC_EUCLIDEAN, lane & 3, FULL);
+        if (row < D.n && (lane & 3) == 0) norms[row] = norm_term(n2, D.metric);
+    }
+}
+
+struct Lock {
+    kg_ctx *c;
+    explicit Lock(kg_ctx *ctx) : c(ctx) { c->mu.lock(); cudaSetDevice(c->device); }
+    ~Lock() { c->mu.unlock(); }
+};
+
+}  // namespace
+
+extern "C" {
+
+void kg_index_params_default(kg_index_params *p) {
+    p->iterations = 30; p->L = 100; p->K = 25; p->S = 10; p->R = 100; p->controls = 100; p->seed = 1998;
+    p->delta = 0.002f; p->recall = 0.99f; p->prune = 0; p->reverse = 0;
+}
+
+void kg_search_params_default(kg_search_params *p) {
+    p->K = 25; p->M = 0; p->P = 100; p->S = 10; p->T = 1; p->epsilon = 1e30f; p->seed = 1998; p->init = 0;
+}
+
+const char *kg_version(void) { return "kgraph-b200-1.0 (sm_100a)"; }
+
+int kg_ctx_create(int device, kg_ctx **out) {
+    if (!out) return KG_E_INVALID;
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || device < 0 || device >= ndev) return KG_E_CUDA;
+    kg_ctx *c = new kg_ctx;
+    c->device = device;
+    cudaSetDevice(device);
+    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreate(&c->ev0)) != cudaSuccess || (e = cudaEventCreate(&c->ev1)) != cudaSuccess ||
+        (e = c->errw.reserve(sizeof(uint32_t))) != cudaSuccess || (e = c->counter.reserve(64)) != cudaSuccess) {
+        delete c;
+        return KG_E_CUDA;
+    }
+    cudaMemset(c->errw.p, 0, sizeof(uint32_t));
+    *out = c;
+    return KG_OK;
+}
+
+void kg_ctx_destroy(kg_ctx *c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    DevBuf *bufs[] = {&c->X, &c->norms, &c->offsets, &c->nbr, &c->nbr_d, &c->Mnode, &c->errw, &c->counter,
+                      &c->visited, &c->qbuf, &c->kbuf, &c->pbuf, &c->seeds, &c->seed_index, &c->init_ids,
+                      &c->out_ids, &c->out_d, &c->out_cnt, &c->out_cost};
+    for (DevBuf *b : bufs) b->release();
+    for (auto &b : c->build_scratch) b.release();
+    cudaEventDestroy(c->ev0);
+    cudaEventDestroy(c->ev1);
+    cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char *kg_last_error(kg_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int kg_last_timing(kg_ctx *ctx, float *build_ms, float *search_ms) {
+    if (!ctx) return KG_E_INVALID;
+    if (build_ms) *build_ms = ctx->last_build_ms;
+    if (search_ms) *search_ms = ctx->last_search_ms;
+    return KG_OK;
+}
+
+int kg_set_data(kg_ctx *ctx, const float *rows, size_t n, size_t d, size_t stride_bytes, int metric) {
+    if (!ctx) return KG_E_INVALID;
+    Lock lk(ctx);
+    if (!rows || n == 0 || d == 0) return set_error(ctx, KG_E_INVALID, "bad array");
+    if (n >= 0x7FFFFFFFull) return set_error(ctx, KG_E_INVALID, "dataset too large (n must be < 2^31)");
+    if (metric < 0 || metric > 2) return set_error(ctx, KG_E_RUNTIME, "metric not supported");
+    if (stride_bytes < d * sizeof(float)) return set_error(ctx, KG_E_INVALID, "bad stride");
+    uint32_t ld = (uint32_t)((d + 15) / 16 * 16);
+    cudaError_t e;
+    if ((e = ctx->X.reserve((size_t)n * ld * sizeof(float))) != cudaSuccess) return cuda_fail(ctx, e, "alloc data");
+    if ((e = ctx->norms.reserve((size_t)n * sizeof(float))) != cudaSuccess) return cuda_fail(ctx, e, "alloc norms");
+    cudaMemsetAsync(ctx->X.p, 0, (size_t)n * ld * sizeof(float), ctx->stream);
+    cudaMemcpyKind kind = is_device_ptr(rows) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    e = cudaMemcpy2DAsync(ctx->X.p, ld * sizeof(float), rows, stride_bytes, d * sizeof(float), n, kind, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "copy data");
+    ctx->n = (uint32_t)n; ctx->d = (uint32_t)d; ctx->ld = ld; ctx->metric = metric;
+    DataView D{ctx->X.as<float>(), ctx->norms.as<float>(), ctx->n, ctx->d, ctx->ld, metric};
+    norms_kernel<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(D, ctx->norms.as<float>());
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "norms");
+    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "set_data");
+    ctx->has_data = true;
+    // A graph from another dataset is not valid for this one.
+    if (ctx->has_graph && ctx->gn > ctx->n) ctx->has_graph = false;
+    return KG_OK;
+}
+
+int kg_graph_size(kg_ctx *ctx, size_t *n, size_t *E) {
+    if (!ctx) return KG_E_INVALID;
+    Lock lk(ctx);
+    if (!ctx->has_graph) return set_error(ctx, KG_E_RUNTIME, "no index");
+    if (n) *n = ctx->gn;
+    if (E) *E = ctx->E;
+    return KG_OK;
+}
+
+int kg_graph_export(kg_ctx *ctx, uint64_t *offsets, uint32_t *ids, float *dists, uint32_t *M) {
+    if (!ctx) return KG_E_INVALID;
+    Lock lk(ctx);
+    if (!ctx->has_graph) return set_error(ctx, KG_E_RUNTIME, "no index");
+    if (dists && ctx->no_dist) return set_error(ctx, KG_E_RUNTIME, "distance information is not available");
+    cudaError_t e = cudaSuccess;
+    if (offsets && e == cudaSuccess)
+        e = cudaMemcpyAsync(offsets, ctx->offsets.p, (ctx->gn + 1) * sizeof(uint64_t), cudaMemcpyDefault, ctx->stream);
+    if (ids && e == cudaSuccess && ctx->E)
+        e = cudaMemcpyAsync(ids, ctx->nbr.p, ctx->E * sizeof(uint32_t), cudaMemcpyDefault, ctx->stream);
+    if (dists && e == cudaSuccess && ctx->E)
+        e = cudaMemcpyAsync(dists, ctx->nbr_d.p, ctx->E * sizeof(float), cudaMemcpyDefault, ctx->stream);
+    if (M && e == cudaSuccess)
+        e = cudaMemcpyAsync(M, ctx->Mnode.p, ctx->gn * sizeof(uint32_t), cudaMemcpyDefault, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "graph export");
+    return KG_OK;
+}
+
+int kg_graph_import(kg_ctx *ctx, size_t n, const uint64_t *offsets, const uint32_t *ids, const float *dists,
+                    const uint32_t *M) {
+    if (!ctx) return KG_E_INVALID;
+    Lock lk(ctx);
+    if (!offsets || !M || n == 0) return set_error(ctx, KG_E_INVALID, "bad graph");
+    std::vector<uint64_t> hoff(n + 1);
+    cudaMemcpy(hoff.data(), offsets, (n + 1) * sizeof(uint64_t), cudaMemcpyDefault);
+    uint64_t E = hoff[n];
+    if (hoff[0] != 0) return set_error(ctx, KG_E_INVALID, "bad graph offsets");
+    for (size_t i = 0; i < n; ++i)
+        if (hoff[i + 1] < hoff[i]) return set_error(ctx, KG_E_INVALID, "bad graph offsets");
+    if (E && !ids) return set_error(ctx, KG_E_INVALID, "bad graph");
+    cudaError_t e;
+    if ((e = ctx->offsets.reserve((n + 1) * sizeof(uint64_t))) != cudaSuccess ||
+        (e = ctx->nbr.reserve(E * sizeof(uint32_t) + 4)) != cudaSuccess ||
+        (e = ctx->nbr_d.reserve(E * sizeof(float) + 4)) != cudaSuccess ||
+        (e = ctx->Mnode.reserve(n * sizeof(uint32_t))) != cudaSuccess)
+        return cuda_fail(ctx, e, "alloc graph");
+    cudaMemcpyAsync(ctx->offsets.p, hoff.data(), (n + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, ctx->stream);
+    if (E) cudaMemcpyAsync(ctx->nbr.p, ids, E * sizeof(uint32_t), cudaMemcpyDefault, ctx->stream);
+    if (E && dists) cudaMemcpyAsync(ctx->nbr_d.p, dists, E * sizeof(float), cudaMemcpyDefault, ctx->stream);
+    cudaMemcpyAsync(ctx->Mnode.p, M, n * sizeof(uint32_t), cudaMemcpyDefault, ctx->stream);
+    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "graph import");
+    ctx->gn = (uint32_t)n;
+    ctx->E = E;
+    ctx->no_dist = dists == nullptr;
+    ctx->has_graph = true;
+    return KG_OK;
+}
+
+int kg_search_batch(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes,
+                    const kg_search_params *params, const uint32_t *K_per_q, const uint32_t *P_per_q,
+                    size_t out_ld, uint32_t *ids, float *dists, uint32_t *counts, float *costs) {
+    if (!ctx) return KG_E_INVALID;
+    Lock lk(ctx);
+    if (!ctx->has_data) return set_error(ctx, KG_E_RUNTIME, "no dataset");
+    if (!params || !ids || !counts) return set_error(ctx, KG_E_INVALID, "bad arguments");
+    if (nq == 0) return KG_OK;
+    if (!queries || q_stride_bytes < ctx->d * sizeof(float)) return set_error(ctx, KG_E_INVALID, "bad query array");
+    const bool graph = ctx->has_graph;
+    if (graph && ctx->gn > ctx->n) return set_error(ctx, KG_E_RUNTIME, "dataset larger than index");
+    if (params->init && params->T > 1) return set_error(ctx, KG_E_RUNTIME, "when init > 0, T must be 1.");
+    const uint32_t N = graph ? ctx->gn : ctx->n;
+    const size_t Q = nq;
+    cudaError_t e;
+
+    // per-query K and P (host copies needed for sizing and the seed table)
+    std::vector<uint32_t> hK, hP;
+    if (K_per_q) {
+        hK.resize(Q);
+        cudaMemcpy(hK.data(), K_per_q, Q * sizeof(uint32_t), cudaMemcpyDefault);
+    }
+    if (P_per_q) {
+        hP.resize(Q);
+        cudaMemcpy(hP.data(), P_per_q, Q * sizeof(uint32_t), cudaMemcpyDefault);
+    }
+    uint32_t Kmax = params->K, Pmax = params->P;
+    if (K_per_q) Kmax = *std::max_element(hK.begin(), hK.end());
+    if (P_per_q) Pmax = *std::max_element(hP.begin(), hP.end());
+    if (Kmax > out_ld) return set_error(ctx, KG_E_INVALID, "out_ld smaller than K");
+    if (params->init && params->init > out_ld) return set_error(ctx, KG_E_INVALID, "init larger than out_ld");
+
+    // without an index every query is a brute-force query (python-api.cpp:303-314)
+    const uint32_t Pforce = graph ? 0u : N;
+    uint32_t effPmax = graph ? Pmax : N;
+    // seed table: for each distinct P < N, T lists of P ids from mt19937(seed)
+    unsigned seed = params->seed;
+    if (seed == 0) seed = (unsigned)time(NULL);
+    std::vector<uint32_t> hseeds, hsidx(graph && params->init == 0 ? Q : 0);
+    if (graph && params->init == 0) {
+        std::map<uint32_t, uint32_t> where;
+        auto add = [&](uint32_t P) {
+            if (where.count(P) || P >= N) return;
+            where[P] = (uint32_t)hseeds.size();
+            std::mt19937 rng(seed);
+            std::vector<uint32_t> tmp(P + 1);
+            for (uint32_t t = 0; t < params->T; ++t) {
+                kgb::gen_random(rng, tmp.data(), P, N);
+                hseeds.insert(hseeds.end(), tmp.begin(), tmp.begin() + P);
+            }
+        };
+        if (P_per_q) for (size_t i = 0; i < Q; ++i) add(hP[i]);
+        else add(params->P);
+        for (size_t i = 0; i < Q; ++i) {
+            uint32_t P = P_per_q ? hP[i] : params->P;
+            hsidx[i] = P >= N ? 0u : where[P];
+        }
+    }
+    if (hseeds.empty()) hseeds.push_back(0);
+    if (hsidx.empty()) hsidx.push_back(0);
+
+    // device buffers
+    const uint32_t ld = ctx->ld;
+    SearchArgs a{};
+    a.D = DataView{ctx->X.as<float>(), ctx->norms.as<float>(), N, ctx->d, ld, ctx->metric};
+    a.offsets = graph ? ctx->offsets.as<uint64_t>() : nullptr;
+    a.nbr = graph ? ctx->nbr.as<uint32_t>() : nullptr;
+    a.Mnode = graph ? ctx->Mnode.as<uint32_t>() : nullptr;
+    a.nq = (uint32_t)Q;
+    a.q_ld = ld;
+    a.K = params->K; a.P = graph ? params->P : Pforce; a.Mp = params->M; a.S = params->S; a.T = params->T;
+    a.init = graph ? params->init : 0u;
+    a.epsilon = params->epsilon;
+    a.out_ld = (uint32_t)out_ld;
+    a.cap = Kmax + effPmax + 1;
+    a.rcap = Kmax + 1;
+    if (search_warp_smem_bytes(ld, a.cap, a.rcap) > 200 * 1024)
+        return set_error(ctx, KG_E_INVALID, "K + P too large for one query's shared-memory pool");
+
+    // queries: use in place when already device rows of ld floats, else stage
+    const bool q_dev = is_device_ptr(queries);
+    if (q_dev && q_stride_bytes == ld * sizeof(float) && (reinterpret_cast<uintptr_t>(queries) & 15) == 0) {
+        a.Q = queries;
+    } else {
+        if ((e = ctx->qbuf.reserve(Q * ld * sizeof(float))) != cudaSuccess) return cuda_fail(ctx, e, "alloc queries");
+        if (ld != ctx->d) cudaMemsetAsync(ctx->qbuf.p, 0, Q * ld * sizeof(float), ctx->stream);
+        e = cudaMemcpy2DAsync(ctx->qbuf.p, ld * sizeof(float), queries, q_stride_bytes, ctx->d * sizeof(float), Q,
+                              q_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "copy queries");
+        a.Q = ctx->qbuf.as<float>();
+    }
+    if (K_per_q) {
+        if ((e = ctx->kbuf.reserve(Q * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc K");
+        cudaMemcpyAsync(ctx->kbuf.p, hK.data(), Q * 4, cudaMemcpyHostToDevice, ctx->stream);
+        a.Kq = ctx->kbuf.as<uint32_t>();
+    }
+    if (P_per_q && graph) {
+        if ((e = ctx->pbuf.reserve(Q * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc P");
+        cudaMemcpyAsync(ctx->pbuf.p, hP.data(), Q * 4, cudaMemcpyHostToDevice, ctx->stream);
+        a.Pq = ctx->pbuf.as<uint32_t>();
+    }
+    if ((e = ctx->seeds.reserve(hseeds.size() * 4)) != cudaSuccess ||
+        (e = ctx->seed_index.reserve(hsidx.size() * 4)) != cudaSuccess)
+        return cuda_fail(ctx, e, "alloc seeds");
+    cudaMemcpyAsync(ctx->seeds.p, hseeds.data(), hseeds.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(ctx->seed_index.p, hsidx.data(), hsidx.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
+    a.seeds = ctx->seeds.as<uint32_t>();
+    a.seed_index = ctx->seed_index.as<uint32_t>();
+
+    // outputs (device in place, or staged)
+    const bool ids_dev = is_device_ptr(ids), d_dev = dists && is_device_ptr(dists), c_dev = is_device_ptr(counts),
+               cost_dev = costs && is_device_ptr(costs);
+    if (!ids_dev) {
+        if ((e = ctx->out_ids.reserve(Q * out_ld * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc out");
+        a.out_ids = ctx->out_ids.as<uint32_t>();
+    } else a.out_ids = ids;
+    if (a.init) {
+        if ((e = ctx->init_ids.reserve(Q * out_ld * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc init");
+        cudaMemcpyAsync(ctx->init_ids.p, ids, Q * out_ld * 4, cudaMemcpyDefault, ctx->stream);
+        a.init_ids = ctx->init_ids.as<uint32_t>();
+    }
+    if (!ids_dev) {   // keep caller's untouched tail entries (the reference leaves them as they were)
+        cudaMemcpyAsync(a.out_ids, ids, Q * out_ld * 4, cudaMemcpyHostToDevice, ctx->stream);
+    }
+    if (dists) {
+        if (!d_dev) {
+            if ((e = ctx->out_d.reserve(Q * out_ld * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc out");
+            a.out_dists = ctx->out_d.as<float>();
+            cudaMemcpyAsync(a.out_dists, dists, Q * out_ld * 4, cudaMemcpyHostToDevice, ctx->stream);
+        } else a.out_dists = dists;
+    }
+    if (!c_dev) {
+        if ((e = ctx->out_cnt.reserve(Q * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc out");
+        a.out_count = ctx->out_cnt.as<uint32_t>();
+    } else a.out_count = counts;
+    if (costs) {
+        if (!cost_dev) {
+            if ((e = ctx->out_cost.reserve(Q * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc out");
+            a.out_cost = ctx->out_cost.as<float>();
+        } else a.out_cost = costs;
+    }
+
+    // visited sets: one per resident warp
+    a.vwords = ((N + 31) / 32 + 3) / 4 * 4;
+    uint32_t slots = search_max_slots(a, ctx->num_sms);
+    if ((e = ctx->visited.reserve((size_t)slots * a.vwords * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc visited");
+    a.visited = ctx->visited.as<uint32_t>();
+    a.visited_slots = slots;
+    a.qcounter = ctx->counter.as<uint32_t>();
+    a.err = ctx->errw.as<uint32_t>();
+    cudaMemsetAsync(a.qcounter, 0, 4, ctx->stream);
+
+    cudaEventRecord(ctx->ev0, ctx->stream);
+    if ((e = launch_search(a, ctx->num_sms, ctx->stream, nullptr)) != cudaSuccess) return cuda_fail(ctx, e, "search launch");
+    cudaEventRecord(ctx->ev1, ctx->stream);
+
+    if (!ids_dev) cudaMemcpyAsync(ids, a.out_ids, Q * out_ld * 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if (dists && !d_dev) cudaMemcpyAsync(dists, a.out_dists, Q * out_ld * 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if (!c_dev) cudaMemcpyAsync(counts, a.out_count, Q * 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if (costs && !cost_dev) cudaMemcpyAsync(costs, a.out_cost, Q * 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "search");
+    cudaEventElapsedTime(&ctx->last_search_ms, ctx->ev0, ctx->ev1);
+    return check_device_error(ctx, "search");
+}
+
+}  // extern "C"

@@ -1,0 +1,81 @@
+// Library context: one GPU, one stream, the dataset and the graph in HBM.
+#pragma once
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+#include "kg_common.cuh"
+#include "../../include/kgraph_b200.h"
+
+namespace kgb {
+
+// A device buffer that only grows.
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    cudaError_t reserve(size_t b) {
+        if (b <= bytes) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        size_t nb = b < 256 ? 256 : b;
+        cudaError_t e = cudaMalloc(&p, nb);
+        if (e == cudaSuccess) bytes = nb;
+        return e;
+    }
+    void release() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
+    template <typename T> T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+struct Error {
+    int code;
+    std::string msg;
+};
+
+}  // namespace kgb
+
+struct kg_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::mutex mu;
+    std::string err;
+    float last_build_ms = 0.f, last_search_ms = 0.f;
+
+    // dataset
+    kgb::DevBuf X, norms;
+    uint32_t n = 0, d = 0, ld = 0;
+    int metric = 0;
+    bool has_data = false;
+
+    // graph, CSR
+    kgb::DevBuf offsets, nbr, nbr_d, Mnode;
+    uint64_t E = 0;
+    uint32_t gn = 0;
+    bool has_graph = false;
+    bool no_dist = false;
+
+    // scratch
+    kgb::DevBuf errw, counter, visited, qbuf, kbuf, pbuf, seeds, seed_index, init_ids, out_ids, out_d,
+        out_cnt, out_cost;
+    std::vector<uint32_t> h_stage_u32;
+
+    kgb::DevBuf build_scratch[24];   // NN-descent state (kg_build.cu)
+};
+
+namespace kgb {
+
+// Helpers shared by the entry-point files.
+int set_error(kg_ctx *ctx, int code, const std::string &msg);
+int cuda_fail(kg_ctx *ctx, cudaError_t e, const char *what);
+bool is_device_ptr(const void *p);
+// Reads and clears the device error word; returns KG_OK or sets the message.
+int check_device_error(kg_ctx *ctx, const char *what);
+// Exact top-K brute force of `nq` dataset rows (LinearSearch, kgraph.cpp:212-229)
+// used for the build's control nodes.
+cudaError_t launch_linear_search(kg_ctx *ctx, const uint32_t *rows, uint32_t nq, uint32_t K, uint32_t *out_ids,
+                                 float *out_d);
+
+}  // namespace kgb

@@ -1,0 +1,343 @@
+// Batched graph-walk search: KGraphImpl::search (kgraph.cpp:423-564) for a
+// whole batch of queries in one persistent launch.
+//
+// Layout.  One warp owns one query at a time and pulls the next query index
+// from a global counter, so queries with uneven K and P balance themselves.
+// The warp keeps the query vector and its candidate pool (K+P+1 entries:
+// dist, id|flag, m|M<<16 -- the reference's NeighborX) in shared memory, and
+// a private N-bit visited set in global memory (the reference's
+// dynamic_bitset, kgraph.cpp:438).
+//
+// Exactness.  The walk is the reference's, step for step: the same P seeds
+// for every query (host mt19937(seed) + GenRandom, kgraph.cpp:444-453), the
+// seed pool sorted by the GNU introsort (kgraph.cpp:476), neighbours visited
+// in adjacency order S at a time, each inserted with UpdateKnnList
+// semantics, k reset to the insert position (kgraph.cpp:478-514).  The
+// distances of one batch of S neighbours are computed in parallel (they are
+// pure), then inserted one by one in order, which is what the reference's
+// interleaved loop produces.  With the canonical distance this reproduces
+// the reference's ids, distances, result count and SearchInfo.cost exactly.
+#include "kg_common.cuh"
+#include "kg_warp.cuh"
+#include "kg_sort.h"
+#include "kg_search.h"
+
+namespace kgb {
+
+namespace {
+
+struct PoolAcc {   // accessor for gnu_sort over the smem pool triples
+    float *d; uint32_t *i; uint32_t *m;
+    struct Rec { float d; uint32_t i, m; };
+    __device__ float key(int x) const { return d[x]; }
+    __device__ void swap(int x, int y) const {
+        float td = d[x]; d[x] = d[y]; d[y] = td;
+        uint32_t ti = i[x]; i[x] = i[y]; i[y] = ti;
+        uint32_t tm = m[x]; m[x] = m[y]; m[y] = tm;
+    }
+    __device__ Rec get(int x) const { return Rec{d[x], i[x], m[x]}; }
+    __device__ void put(int x, Rec r) const { d[x] = r.d; i[x] = r.i; m[x] = r.m; }
+    __device__ float rkey(Rec r) const { return r.d; }
+};
+
+struct WarpSmem {
+    float *q;          // ld floats
+    float *pd;         // cap
+    uint32_t *pid;     // cap   id | FLAG_BIT
+    uint32_t *pm;      // cap   m | (M << 16)
+    float *rd;         // rcap  (T > 1 result merge)
+    uint32_t *rid;     // rcap
+    float *cd;         // 32    batch distances
+    uint32_t *cid;     // 32    batch ids
+    uint32_t *cM;      // 32    batch actual_M
+};
+
+__device__ __forceinline__ WarpSmem carve(char *base, const SearchArgs &a) {
+    WarpSmem s;
+    char *p = base;
+    s.q = reinterpret_cast<float *>(p); p += sizeof(float) * a.D.ld;
+    s.pd = reinterpret_cast<float *>(p); p += sizeof(float) * a.cap;
+    s.pid = reinterpret_cast<uint32_t *>(p); p += sizeof(uint32_t) * a.cap;
+    s.pm = reinterpret_cast<uint32_t *>(p); p += sizeof(uint32_t) * a.cap;
+    s.rd = reinterpret_cast<float *>(p); p += sizeof(float) * a.rcap;
+    s.rid = reinterpret_cast<uint32_t *>(p); p += sizeof(uint32_t) * a.rcap;
+    s.cd = reinterpret_cast<float *>(p); p += sizeof(float) * 32;
+    s.cid = reinterpret_cast<uint32_t *>(p); p += sizeof(uint32_t) * 32;
+    s.cM = reinterpret_cast<uint32_t *>(p);
+    return s;
+}
+
+// actual_M (kgraph.cpp:284-286) as stored in NeighborX::M (uint16_t).
+__device__ __forceinline__ uint32_t actual_M(const SearchArgs &a, uint32_t pM, uint32_t id) {
+    uint32_t deg = (uint32_t)(a.offsets[id + 1] - a.offsets[id]);
+    return min(max(a.Mnode[id], pM), deg) & 0xFFFFu;
+}
+
+// Distances for cnt candidates cid[0..cnt) -> cd[], 8 per pass (4-lane groups).
+__device__ __forceinline__ void batch_dist(const SearchArgs &a, const WarpSmem &s, float qn, uint32_t cnt,
+                                           int lane) {
+    const int g = lane >> 2, t = lane & 3;
+    for (uint32_t base = 0; base < cnt; base += 8) {
+        uint32_t c = base + g;
+        uint32_t id = c < cnt ? s.cid[c] : 0u;
+        float dd = query_dist(a.D, s.q, qn, id, t, FULL);
+        if (c < cnt && t == 0) s.cd[c] = dd;
+    }
+    __syncwarp();
+}
+
+// SearchOracle::search (kgraph.cpp:231-252) by one warp: every row in id
+// order, epsilon filter, sorted insert into K slots (+1 overflow).
+__device__ uint32_t warp_bruteforce(const SearchArgs &a, const WarpSmem &s, float qn, uint32_t K, int lane) {
+    const uint32_t N = a.D.n;
+    uint32_t L = 0;
+    for (uint32_t base = 0; base < N; base += 32) {
+        uint32_t cnt = min(32u, N - base);
+        if (lane < (int)cnt) s.cid[lane] = base + lane;
+        __syncwarp();
+        batch_dist(a, s, qn, cnt, lane);
+        for (uint32_t c = 0; c < cnt; ++c) {
+            float dd = s.cd[c];
+            if (dd > a.epsilon) continue;
+            if (L == K && (K == 0 || dd >= s.pd[K - 1])) continue;   // would land at slot K
+            warp_update_knn(s.pd, s.pid, (uint32_t *)nullptr, L, dd, base + c, 0u, lane);
+            if (L < K) ++L;
+        }
+        __syncwarp();
+    }
+    return L;
+}
+
+__device__ __forceinline__ bool visited_test_set(uint32_t *vis, uint32_t id) {
+    uint32_t bit = 1u << (id & 31);
+    uint32_t old = atomicOr(vis + (id >> 5), bit);
+    return (old & bit) != 0;
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(256) search_kernel(SearchArgs a) {
+    extern __shared__ __align__(16) char smem[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const uint32_t slot = blockIdx.x * a.warps_per_block + wib;
+    WarpSmem s = carve(smem + (size_t)wib * a.warp_smem_bytes, a);
+    uint32_t *vis = a.visited + (size_t)slot * a.vwords;
+    const uint32_t N = a.D.n;
+
+    for (;;) {
+        uint32_t qi = 0;
+        if (lane == 0) qi = atomicAdd(a.qcounter, 1u);
+        qi = __shfl_sync(FULL, qi, 0);
+        if (qi >= a.nq) break;
+        const uint32_t K = a.Kq ? a.Kq[qi] : a.K;
+        const uint32_t P = a.Pq ? a.Pq[qi] : a.P;
+        const uint32_t T = a.T;
+        const uint32_t S = a.S;
+        const uint32_t cap = K + P + 1;   // knn.size(), kgraph.cpp:434
+
+        // query -> smem, and its norm term (SearchOracle ctor, python-api.cpp:98-101)
+        const float *qg = a.Q + (size_t)qi * a.q_ld;
+        for (uint32_t x = lane * 4; x < a.D.ld; x += 128)
+            *reinterpret_cast<float4 *>(s.q + x) = ld4(qg + x);
+        __syncwarp();
+        float qn = 0.f;
+        if (a.D.metric != METRIC_L2SQR) {
+            float n2 = group4_raw(s.q, s.q, a.D.d, METRIC_EUCLIDEAN, lane & 3, FULL);
+            qn = norm_term(n2, a.D.metric);
+        }
+
+        uint32_t count = 0;
+        float cost = 0.f;
+        uint32_t *out_i = a.out_ids + (size_t)qi * a.out_ld;
+        float *out_d = a.out_dists ? a.out_dists + (size_t)qi * a.out_ld : nullptr;
+
+        if (P >= N) {   // kgraph.cpp:427-433: brute force, cost 1
+            count = warp_bruteforce(a, s, qn, K, lane);
+            for (uint32_t k = lane; k < count; k += 32) {
+                out_i[k] = s.pid[k] & ID_MASK;
+                if (out_d) out_d[k] = s.pd[k];
+            }
+            if (lane == 0) { a.out_count[qi] = count; if (a.out_cost) a.out_cost[qi] = 1.0f; }
+            __syncwarp();
+            continue;
+        }
+        if (a.init && !(a.init < K)) {   // kgraph.cpp:463
+            if (lane == 0) { raise_error(a.err, ERR_INIT_K); a.out_count[qi] = 0; }
+            __syncwarp();
+            continue;
+        }
+
+        for (uint32_t w = lane * 4; w < a.vwords; w += 128)
+            *reinterpret_cast<uint4 *>(vis + w) = make_uint4(0u, 0u, 0u, 0u);
+        __syncwarp();
+
+        uint32_t n_comps = 0;
+        uint32_t rn = 0;          // results.size() - 1
+        bool have_results = false;
+        for (uint32_t trial = 0; trial < T; ++trial) {
+            uint32_t L = 0;
+            if (a.init == 0) {
+                const uint32_t *seeds = a.seeds + a.seed_index[qi] + (size_t)trial * P;
+                // kgraph.cpp:454-459: keep seeds not visited by an earlier trial
+                for (uint32_t base = 0; base < P; base += 32) {
+                    uint32_t j = base + lane;
+                    uint32_t sid = j < P ? seeds[j] : 0u;
+                    bool keep = j < P && !((__ldcg(vis + (sid >> 5)) >> (sid & 31)) & 1u);
+                    unsigned m = __ballot_sync(FULL, keep);
+                    if (keep) s.pid[L + __popc(m & ((1u << lane) - 1u))] = sid;
+                    L += __popc(m);
+                }
+            } else {
+                L = a.init;
+                const uint32_t *init = a.init_ids + (size_t)qi * a.out_ld;
+                for (uint32_t j = lane; j < L; j += 32) s.pid[j] = init[j];
+            }
+            __syncwarp();
+            // kgraph.cpp:468-475: mark, flag, distance, m = 0, M = actual_M
+            for (uint32_t base = 0; base < L; base += 32) {
+                uint32_t j = base + lane;
+                uint32_t id = j < L ? s.pid[j] : 0u;
+                bool bad = j < L && id >= N;
+                if (__any_sync(FULL, bad)) {
+                    if (lane == 0) raise_error(a.err, ERR_BAD_ID);
+                }
+                if (j < L && !bad) {
+                    atomicOr(vis + (id >> 5), 1u << (id & 31));
+                    s.pm[j] = actual_M(a, a.Mp, id) << 16;
+                }
+                __syncwarp();
+                uint32_t cnt = min(32u, L - base);
+                if (j < L) s.cid[lane] = bad ? 0u : id;
+                __syncwarp();
+                batch_dist(a, s, qn, cnt, lane);
+                if (j < L) { s.pd[j] = s.cd[lane]; s.pid[j] = id | FLAG_BIT; }
+                __syncwarp();
+            }
+            // kgraph.cpp:476: std::sort by dist (GNU introsort order for ties)
+            if (lane == 0) {
+                PoolAcc acc{s.pd, s.pid, s.pm};
+                gnu_sort(acc, 0, (int)L);
+            }
+            __syncwarp();
+
+            uint32_t k = 0;
+            while (true) {
+                k = warp_next_flagged(s.pid, k, L, lane);
+                if (k >= L) break;
+                const uint32_t idf = s.pid[k];
+                const uint32_t mM = s.pm[k];
+                const uint32_t beginM = mM & 0xFFFFu, eM = mM >> 16;
+                uint32_t endM = beginM + S;
+                uint32_t nidf = idf;
+                if (endM > eM) { nidf = idf & ID_MASK; endM = eM; }   // kgraph.cpp:487-490
+                __syncwarp();
+                if (lane == 0) { s.pid[k] = nidf; s.pm[k] = (endM & 0xFFFFu) | (eM << 16); }
+                __syncwarp();
+                const uint32_t node = idf & ID_MASK;
+                const uint64_t nb = a.offsets[node];
+                for (uint32_t m0 = beginM; m0 < endM; m0 += 32) {
+                    const uint32_t cnt = min(32u, endM - m0);
+                    bool act = lane < (int)cnt;
+                    uint32_t id = act ? a.nbr[nb + m0 + lane] : 0xFFFFFFFFu;
+                    bool bad = act && id >= N;
+                    if (__any_sync(FULL, bad)) { if (lane == 0) raise_error(a.err, ERR_BAD_ID); }
+                    act = act && !bad;
+                    // first occurrence within this chunk, in adjacency order
+                    unsigned same = __match_any_sync(FULL, id);
+                    bool first = act && ((__ffs(same & __ballot_sync(FULL, act)) - 1) == lane);
+                    bool isnew = false;
+                    if (first) isnew = !visited_test_set(vis, id);
+                    unsigned nm = __ballot_sync(FULL, isnew);
+                    uint32_t nnew = __popc(nm);
+                    if (nnew == 0) continue;
+                    n_comps += nnew;
+                    uint32_t pos = __popc(nm & ((1u << lane) - 1u));
+                    if (isnew) { s.cid[pos] = id; s.cM[pos] = actual_M(a, a.Mp, id); }
+                    __syncwarp();
+                    batch_dist(a, s, qn, nnew, lane);
+                    for (uint32_t c = 0; c < nnew; ++c) {
+                        const float dd = s.cd[c];
+                        const uint32_t cidv = s.cid[c];
+                        uint32_t r = warp_update_knn(s.pd, s.pid, s.pm, L, dd, cidv | FLAG_BIT, 0u, lane);
+                        if (L + 1 < cap) ++L;
+                        if (r < L) {
+                            if (lane == 0) s.pm[r] = (s.pm[r] & 0xFFFFu) | (s.cM[c] << 16);
+                            if (r < k) k = r;
+                        }
+                        __syncwarp();
+                    }
+                }
+            }
+            if (L > K) L = K;   // kgraph.cpp:515
+            if (!have_results) {
+                for (uint32_t j = lane; j < L; j += 32) { s.rd[j] = s.pd[j]; s.rid[j] = s.pid[j]; }
+                rn = L;
+                have_results = true;
+                __syncwarp();
+            } else {   // kgraph.cpp:521-528
+                for (uint32_t l = 0; l < L; ++l) {
+                    uint32_t r = warp_update_knn(s.rd, s.rid, (uint32_t *)nullptr, rn, s.pd[l], s.pid[l], 0u, lane);
+                    if (r < rn + 1 && rn + 1 < K + 1) ++rn;
+                }
+            }
+        }
+        // kgraph.cpp:531-540: drop the spare slot, epsilon filter
+        count = rn;
+        for (uint32_t base = 0; base < count; base += 32) {
+            uint32_t j = base + lane;
+            unsigned m = __ballot_sync(FULL, j < count && s.rd[j] > a.epsilon);
+            if (m) { count = base + __ffs(m) - 1; break; }
+        }
+        for (uint32_t k = lane; k < count; k += 32) {
+            out_i[k] = s.rid[k] & ID_MASK;
+            if (out_d) out_d[k] = s.rd[k];
+        }
+        cost = __fdiv_rn((float)n_comps, (float)N);   // kgraph.cpp:561
+        if (lane == 0) { a.out_count[qi] = count; if (a.out_cost) a.out_cost[qi] = cost; }
+        __syncwarp();
+    }
+}
+
+size_t search_warp_smem_bytes(uint32_t ld, uint32_t cap, uint32_t rcap) {
+    size_t b = sizeof(float) * ld + 12ull * cap + 8ull * rcap + 12ull * 32;
+    return (b + 15) & ~size_t(15);
+}
+
+cudaError_t launch_search(SearchArgs &a, int num_sms, cudaStream_t st, uint32_t *grid_out) {
+    a.warp_smem_bytes = (uint32_t)search_warp_smem_bytes(a.D.ld, a.cap, a.rcap);
+    // Warps per block: as many as fit 200 KB of shared memory, at most 8.
+    uint32_t wpb = 8;
+    while (wpb > 1 && (size_t)wpb * a.warp_smem_bytes > 200 * 1024) wpb >>= 1;
+    if ((size_t)wpb * a.warp_smem_bytes > 227 * 1024) return cudaErrorInvalidValue;
+    a.warps_per_block = wpb;
+    size_t smem = (size_t)wpb * a.warp_smem_bytes;
+    cudaError_t e = cudaFuncSetAttribute(search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_kernel, wpb * 32, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    uint32_t grid = (uint32_t)(num_sms * per_sm);
+    uint32_t need = (a.nq + wpb - 1) / wpb;
+    if (grid > need) grid = need;
+    if (grid < 1) grid = 1;
+    if (grid_out) *grid_out = grid;
+    if (grid * wpb > a.visited_slots) return cudaErrorInvalidValue;
+    search_kernel<<<grid, wpb * 32, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+uint32_t search_max_slots(const SearchArgs &a, int num_sms) {
+    size_t wb = search_warp_smem_bytes(a.D.ld, a.cap, a.rcap);
+    uint32_t wpb = 8;
+    while (wpb > 1 && (size_t)wpb * wb > 200 * 1024) wpb >>= 1;
+    size_t smem = (size_t)wpb * wb;
+    cudaFuncSetAttribute(search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_kernel, wpb * 32, smem);
+    if (per_sm < 1) per_sm = 1;
+    return (uint32_t)(num_sms * per_sm) * wpb;
+}
+
+}  // namespace kgb

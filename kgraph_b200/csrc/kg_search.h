@@ -1,0 +1,40 @@
+// Launch interface of the batched graph-walk search kernel (kg_search.cu).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "kg_common.cuh"
+
+namespace kgb {
+
+struct SearchArgs {
+    DataView D;
+    const uint64_t *offsets;    // CSR graph: n+1 offsets
+    const uint32_t *nbr;        // neighbour ids
+    const uint32_t *Mnode;      // per-node M (KGraphImpl::M)
+    const float *Q;             // queries, nq rows of q_ld (= D.ld) floats
+    uint32_t q_ld, nq;
+    const uint32_t *Kq, *Pq;    // optional per-query K and P (null: use K, P)
+    uint32_t K, P, Mp, S, T, init;
+    float epsilon;
+    const uint32_t *seeds;      // concatenated seed lists (T lists of P ids per distinct P)
+    const uint32_t *seed_index; // per query: offset of its trial-0 seed list in `seeds`
+    const uint32_t *init_ids;   // init > 0: nq rows of out_ld ids
+    uint32_t *out_ids;          // nq rows of out_ld
+    float *out_dists;           // optional
+    uint32_t *out_count;        // nq
+    float *out_cost;            // optional, SearchInfo.cost
+    uint32_t out_ld;
+    uint32_t *visited;          // visited_slots x vwords words
+    uint32_t vwords, visited_slots;
+    uint32_t *qcounter;         // zeroed before launch
+    uint32_t *err;              // device error word
+    uint32_t cap, rcap;         // smem capacities: max(K+P+1), max(K+1)
+    uint32_t warps_per_block, warp_smem_bytes;   // filled by launch_search
+};
+
+size_t search_warp_smem_bytes(uint32_t ld, uint32_t cap, uint32_t rcap);
+// Upper bound of concurrently resident warps (= visited slots needed).
+uint32_t search_max_slots(const SearchArgs &a, int num_sms);
+cudaError_t launch_search(SearchArgs &a, int num_sms, cudaStream_t st, uint32_t *grid_out);
+
+}  // namespace kgb

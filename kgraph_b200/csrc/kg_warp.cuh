@@ -1,0 +1,83 @@
+// Warp-cooperative primitives over sorted (dist, id) lists held in shared or
+// global memory: the sorted insert with the reference's duplicate rule, and
+// the next-flagged scan of the search walk.
+#pragma once
+#include "kg_common.cuh"
+
+namespace kgb {
+
+constexpr unsigned FULL = 0xFFFFFFFFu;
+
+// Number of entries in the sorted prefix pd[0, L) with pd[j] <= d, i.e. the
+// position UpdateKnnListHelper (kgraph.cpp:180-185) inserts at: after every
+// entry of equal distance.  Two probe rounds: 32 evenly spaced probes locate
+// the segment, then the segment is counted 32 at a time.
+template <typename P>
+__device__ __forceinline__ uint32_t warp_upper_bound(P pd, uint32_t L, float d, int lane) {
+    if (L == 0) return 0;
+    const uint32_t seg = (L + 31) >> 5;
+    const uint32_t probe = (uint32_t)lane * seg;
+    bool le = probe < L && pd[probe] <= d;
+    uint32_t c = __popc(__ballot_sync(FULL, le));
+    if (c == 0) return 0;
+    uint32_t lo = (c - 1) * seg + 1;
+    uint32_t hi = min(c * seg, L);
+    uint32_t i = lo;
+    for (uint32_t base = lo; base < hi; base += 32) {
+        uint32_t j = base + lane;
+        bool b = j < hi && pd[j] <= d;
+        i += __popc(__ballot_sync(FULL, b));
+    }
+    return i;
+}
+
+// True when an entry with distance == d and id == id (flag bit ignored) sits
+// in the run of equal distances that ends at position i-1 (kgraph.cpp:187-193).
+template <typename P, typename I>
+__device__ __forceinline__ bool warp_dup_before(P pd, I pid, uint32_t i, float d, uint32_t id, int lane) {
+    for (int base = (int)i - 32;; base -= 32) {
+        int j = base + lane;
+        bool eq = j >= 0 && j < (int)i && pd[j] == d;
+        bool hit = eq && ((pid[j] & ID_MASK) == (id & ID_MASK));
+        if (__any_sync(FULL, hit)) return true;
+        // The run continues below this chunk only if the chunk's first entry is still equal.
+        bool cont = base > 0 && pd[base] == d;
+        if (!__shfl_sync(FULL, cont, 0)) return false;
+    }
+}
+
+// UpdateKnnListHelper (kgraph.cpp:176-202) by one warp over parallel arrays
+// pd/pid/(pm) holding a sorted list of length L with room for entry L.
+// Returns the insert position, L + 1 for a duplicate.  pm may be null.
+template <typename PD, typename PI>
+__device__ __forceinline__ uint32_t warp_update_knn(PD pd, PI pid, uint32_t *pm, uint32_t L, float d,
+                                                    uint32_t idf, uint32_t mv, int lane) {
+    uint32_t i = warp_upper_bound(pd, L, d, lane);
+    if (warp_dup_before(pd, pid, i, d, idf, lane)) return L + 1;
+    for (int top = (int)L - 1; top >= (int)i; top -= 32) {
+        int j = top - lane;
+        float dv = 0.f;
+        uint32_t iv = 0, mvv = 0;
+        bool act = j >= (int)i;
+        if (act) { dv = pd[j]; iv = pid[j]; if (pm) mvv = pm[j]; }
+        __syncwarp();
+        if (act) { pd[j + 1] = dv; pid[j + 1] = iv; if (pm) pm[j + 1] = mvv; }
+        __syncwarp();
+    }
+    if (lane == 0) { pd[i] = d; pid[i] = idf; if (pm) pm[i] = mv; }
+    __syncwarp();
+    return i;
+}
+
+// First index >= k in [0, L) whose flag bit is set; L if none.
+__device__ __forceinline__ uint32_t warp_next_flagged(const uint32_t *pid, uint32_t k, uint32_t L, int lane) {
+    for (uint32_t base = k; base < L; base += 32) {
+        uint32_t j = base + lane;
+        bool f = j < L && (pid[j] & FLAG_BIT);
+        unsigned m = __ballot_sync(FULL, f);
+        if (m) return base + __ffs(m) - 1;
+    }
+    return L;
+}
+
+}  // namespace kgb

@@ -37,6 +37,8 @@ float dot_impl(const float *a, const float *b, unsigned d) {
     for (; i < vs; i += 16)
         for (int l = 0; l < 16; ++l) acc[l] = acc[l] + a[i + l] * b[i + l];
     float r = reduce16(acc);
+    if (d - i >= 8)   // the compiler vectorises 8 tail products: rounded, added in order
+        for (unsigned e = i + 8; i < e; ++i) r = r + a[i] * b[i];
     for (; i < d; ++i) r = std::fma(a[i], b[i], r);
     return r;
 }
@@ -48,6 +50,8 @@ float norm2_impl(const float *a, unsigned d) {
     for (; i < vs; i += 16)
         for (int l = 0; l < 16; ++l) acc[l] = acc[l] + a[i + l] * a[i + l];
     float r = reduce16(acc);
+    if (d - i >= 8)
+        for (unsigned e = i + 8; i < e; ++i) r = r + a[i] * a[i];
     for (; i < d; ++i) r = std::fma(a[i], a[i], r);
     return r;
 }
@@ -62,6 +66,11 @@ float l2sqr_impl(const float *a, const float *b, unsigned d) {
             acc[l] = acc[l] + t * t;
         }
     float r = reduce16(acc);
+    if (d - i >= 8)
+        for (unsigned e = i + 8; i < e; ++i) {
+            float t = a[i] - b[i];
+            r = r + t * t;
+        }
     for (; i < d; ++i) {
         float t = a[i] - b[i];
         r = std::fma(t, t, r);

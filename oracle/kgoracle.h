@@ -18,8 +18,10 @@
  * as its -O3 build evaluates them (measured bit for bit against oracle/_ref):
  * 16 lanes, lane l accumulates elements l, l+16, ... as a rounded product
  * then a rounded add (the vector intrinsics are not contracted); then the
- * xsimd avx512f reduce_add tree; then the scalar tail (D % 16 elements) with
- * a FUSED multiply-add per element (GCC contracts the scalar `acc += a*b`).
+ * xsimd avx512f reduce_add tree; then the scalar tail (D % 16 elements),
+ * added in order: when the tail has 8 or more elements GCC vectorises the
+ * first 8 products (rounded products, in-order adds); every other tail
+ * element is a FUSED multiply-add (GCC contracts the scalar `acc += a*b`).
  * The angular denominator n_i*n_j + FLT_EPSILON is fused the same way.
  */
 #ifndef KGORACLE_H

@@ -260,9 +260,12 @@ class RefLib:
         return ids, dists, cnt, cost
 
 
-def read_index(path):
+def read_index(path_or_bytes):
     """Parses the reference's binary index file (kgraph.cpp:291-331) into a Graph."""
-    raw = open(path, "rb").read()
+    if isinstance(path_or_bytes, (bytes, bytearray, np.ndarray)):
+        raw = bytes(path_or_bytes)
+    else:
+        raw = open(path_or_bytes, "rb").read()
     if raw[:8] != b"KNNGRAPH":
         raise ValueError("bad magic")
     version, cap, n = np.frombuffer(raw, np.uint32, 3, 8)
