@@ -1,0 +1,364 @@
+"""Benchmark: NN-descent build seconds and batched graph-walk search QPS at
+recall@10 >= 0.95 on one B200, against the reference's CPU path.
+
+Workload (the 1M x 128 configuration): N = 1,000,000 base vectors, D = 128,
+float32 non-negative integers from a 256-centre Gaussian mixture (centre
+coordinates uniform in [0, 128), per-dimension std 20, clipped at 0 and
+rounded), euclidean (the Python oracle's half squared L2); graph built with
+K=50, L=100, S=12, R=100, reverse=-1; 10,000 queries from the same mixture.
+Synthetic data generated from fixed seeds (data 1, queries from the same
+stream); no dataset files are read.
+
+A step is one batched search of the 10,000 queries at K=10 and the smallest
+P of a fixed ladder whose recall@10 (tie-aware, against an exact FP64
+brute force on the GPU) reaches 0.95.  `value` is queries/s with queries and
+outputs resident in HBM; `e2e` is the same through the public C-ABI call with
+host buffers (query upload and result download inside the timed region).
+The dataset (512 MB) is larger than L2 and L2 is also flushed between timed
+steps.  Build seconds are reported in `build`.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun every rank builds its own replica and searches its own 10,000
+queries (replicas only: search shards by query, no collective on the data
+path); value = all ranks' queries / max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "NN-descent build sec & search QPS @ recall@10≥0.95; BF16/router vs FP32 GPU"
+UNIT = "queries/s"
+N_BASE, DIM, N_CENTRES, N_QUERIES = 1_000_000, 128, 256, 10_000
+BUILD = dict(K=50, L=100, S=12, R=100, iterations=30, reverse=-1)
+P_LADDER = [100, 200, 300, 500, 700, 1000, 1500, 2000, 3000]
+TARGET = 0.95
+
+
+def make_data(n=N_BASE, nq=N_QUERIES, d=DIM, centres=N_CENTRES, seed=1, rank=0):
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(0, 128, (centres, d))
+    X = np.empty((n, d), np.float32)
+    step = 200_000
+    for a in range(0, n, step):
+        b = min(n, a + step)
+        lab = rng.integers(0, centres, b - a)
+        X[a:b] = np.round(np.maximum(c[lab] + rng.normal(0, 20, (b - a, d)), 0))
+    qr = np.random.default_rng(2 + 1000 * rank)
+    lab = qr.integers(0, centres, nq)
+    Q = np.round(np.maximum(c[lab] + qr.normal(0, 20, (nq, d)), 0)).astype(np.float32)
+    return X, Q
+
+
+def exact_topk_fp64(Xt, Qt, K, torch):
+    """Exact K-NN by FP64 GEMM on the GPU (the recall judge; integer data is exact in FP64)."""
+    xn = (Xt * Xt).sum(1)
+    out_d, out_i = [], []
+    for a in range(0, Qt.shape[0], 500):
+        q = Qt[a:a + 500]
+        d = xn[None, :] - 2.0 * (q @ Xt.T) + (q * q).sum(1)[:, None]
+        v, i = torch.topk(d, K, dim=1, largest=False)
+        out_d.append(v)
+        out_i.append(i)
+    return torch.cat(out_d), torch.cat(out_i)
+
+
+def recall_at(ids, Xt, Qt, gt_d, K, torch):
+    """Tie-aware recall@K: returned ids whose exact distance is <= the exact K-th."""
+    idx = torch.as_tensor(ids[:, :K].astype(np.int64), device=Xt.device)
+    tot = 0
+    for a in range(0, Qt.shape[0], 1000):
+        x = Xt[idx[a:a + 1000]]                     # [b, K, d]
+        q = Qt[a:a + 1000][:, None, :]
+        dd = ((x - q) ** 2).sum(2)
+        tot += int((dd <= gt_d[a:a + 1000, K - 1:K] + 1e-9).sum())
+    return tot / (Qt.shape[0] * K)
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(2)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = [r for r in self.rows if len(r) >= 7]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[3 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": float(rows[0][1]),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def reference_cpu_search(X, Q, index_path, K, P, threads=0):
+    """The reference's own CPU search (oracle/_ref, python-api.cpp) over an index file."""
+    from oracle import kgoracle as ko
+    kg = ko.load_reference_module()
+    g = kg.KGraph(X, "euclidean")
+    g.load(index_path)
+    t0 = time.perf_counter()
+    ids = g.search(Q, K=K, P=P)
+    return ids, time.perf_counter() - t0
+
+
+def run_reference_arm(args, rank, world):
+    """--impl reference: the reference's CPU build and search on the host cores."""
+    if rank != 0:
+        return
+    from oracle import kgoracle as ko
+    if not ko.reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference not compiled (oracle/_ref missing)"}))
+        return
+    kg = ko.load_reference_module()
+    cores = os.cpu_count()
+    X, Q = make_data()
+    t0 = time.perf_counter()
+    g = kg.KGraph(X, "euclidean")
+    g.build(**{k: v for k, v in BUILD.items() if k != "R"})
+    build_s = time.perf_counter() - t0
+    P = args.ref_P
+    sample = Q[: args.ref_queries]
+    for _ in range(args.warmup):
+        g.search(sample[:100], K=10, P=P)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ids = g.search(sample, K=10, P=P)
+        times.append(time.perf_counter() - t0)
+    qps = len(sample) * len(times) / sum(times)
+    import torch
+    rec = None
+    if torch.cuda.is_available():
+        Xt = torch.as_tensor(X, dtype=torch.float64, device="cuda")
+        Qt = torch.as_tensor(sample, dtype=torch.float64, device="cuda")
+        gd, _ = exact_topk_fp64(Xt, Qt, 10, torch)
+        rec = recall_at(ids, Xt, Qt, gd, 10, torch)
+    line = {"metric": METRIC, "value": qps, "unit": UNIT, "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sum(times) / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "recall@10": rec,
+            "config": {"workload": "1M x 128 mixture (256 centres), K=10 search, P=%d" % P, "P": P,
+                       "queries_per_step": len(sample), "build": BUILD},
+            "build": {"seconds": build_s, "threads": cores},
+            "cpu_baseline": {"value": qps, "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": "%d of the 10k queries per step, K=10, P=%d, on the reference's own "
+                                       "1M-node graph" % (len(sample), P)},
+            "e2e": {"value": qps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=N_BASE)
+    ap.add_argument("--ref-P", type=int, default=1000)
+    ap.add_argument("--ref-queries", type=int, default=2000)
+    ap.add_argument("--cpu-queries", type=int, default=1000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    from kgraph_b200 import capi
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    X, Q = make_data(n=args.n, rank=rank)
+    ctx = capi.Context(local)
+    capi.set_verbosity(0)
+    ctx.set_data(X, "euclidean")
+    # build (timed on the device by the library's own CUDA events)
+    t0 = time.perf_counter()
+    info = ctx.build(**BUILD)
+    build_wall = time.perf_counter() - t0
+    build_ms, _ = ctx.timing()
+
+    # recall ladder on the GPU-built graph; FP64 ground truth on the GPU
+    Xt = torch.as_tensor(X, dtype=torch.float64, device="cuda")
+    Qt = torch.as_tensor(Q, dtype=torch.float64, device="cuda")
+    gt_d, gt_i = exact_topk_fp64(Xt, Qt, 100, torch)
+    ladder = {}
+    P_star = P_LADDER[-1]
+    for P in P_LADDER:
+        ids, _, _, _ = ctx.search(Q, K=10, P=P)
+        ladder[P] = recall_at(ids, Xt, Qt, gt_d, 10, torch)
+        if ladder[P] >= TARGET:
+            P_star = P
+            break
+    ids100, _, _, _ = ctx.search(Q, K=100, P=max(P_star, 100))
+    recall100 = recall_at(ids100, Xt, Qt, gt_d, 100, torch)
+    del Xt
+
+    # device-resident timing (value)
+    q_dev = torch.empty((N_QUERIES, ((DIM + 15) // 16) * 16), dtype=torch.float32, device="cuda")
+    q_dev[:, :DIM] = torch.as_tensor(Q, device="cuda")
+    out_i = torch.empty((N_QUERIES, 10), dtype=torch.int32, device="cuda")
+    out_d = torch.empty((N_QUERIES, 10), dtype=torch.float32, device="cuda")
+    out_c = torch.empty((N_QUERIES,), dtype=torch.int32, device="cuda")
+    params = capi.SearchParams(10, 0, P_star, 10, 1, 1e30, 1998, 0)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step_dev():
+        ctx.search_raw(capi._ptr(q_dev), N_QUERIES, q_dev.stride(0) * 4, params, None, None, 10,
+                       capi._ptr(out_i), capi._ptr(out_d), capi._ptr(out_c), None)
+        return ctx.timing()[1]
+
+    for _ in range(args.warmup):
+        step_dev()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    step_ms = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)                 # L2 flush between timed steps
+            torch.cuda.synchronize()
+            step_ms.append(step_dev())
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    evals, adj = ctx.search_work()
+    tot_ms = sum(step_ms)
+    t = torch.tensor([tot_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    tot_ms_max = float(t.item())
+    value = N_QUERIES * world * args.steps / (tot_ms_max / 1000)
+
+    # end to end through the C-ABI with host buffers
+    Qh = np.ascontiguousarray(Q)
+    hi = np.zeros((N_QUERIES, 10), np.uint32)
+    hd = np.zeros((N_QUERIES, 10), np.float32)
+    hc = np.zeros(N_QUERIES, np.uint32)
+    for _ in range(args.warmup):
+        ctx.search_raw(capi._ptr(Qh), N_QUERIES, Qh.strides[0], params, None, None, 10, capi._ptr(hi), capi._ptr(hd),
+                       capi._ptr(hc), None)
+    e2e_ms = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.search_raw(capi._ptr(Qh), N_QUERIES, Qh.strides[0], params, None, None, 10, capi._ptr(hi), capi._ptr(hd),
+                       capi._ptr(hc), None)
+        e2e_ms.append(1000 * (time.perf_counter() - t0))
+    t = torch.tensor([sum(e2e_ms)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e = N_QUERIES * world * args.steps / (float(t.item()) / 1000)
+
+    # roofline of the search kernel: algorithmic bytes per launch / launch time
+    bytes_per_launch = evals * (DIM * 4 + 4) + adj * 4
+    achieved = bytes_per_launch / (tot_ms / args.steps / 1000) / 1e9
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import kgoracle as ko
+            if ko.reference_available():
+                import tempfile
+                with tempfile.TemporaryDirectory() as tmp:
+                    p = os.path.join(tmp, "g.idx")
+                    off, gi, gd, gM = ctx.graph()
+                    ctx_save(p, off, gi, gd, gM)
+                    sample = Q[: args.cpu_queries]
+                    _, secs = reference_cpu_search(X, sample, p, 10, P_star)
+                    cpu = {"value": len(sample) / secs, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                           "sample": "%d queries, K=10, P=%d, reference CPU search (oracle/_ref, OpenMP over "
+                                     "queries) on the same GPU-built graph" % (len(sample), P_star)}
+        except Exception as e:   # reported, not fatal
+            cpu = {"error": str(e)[:200]}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": tot_ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "1M x 128 mixture (256 centres), 10k queries, K=10, P=%d" % P_star,
+                           "N": args.n, "D": DIM, "queries": N_QUERIES, "K": 10, "P": P_star, "build": BUILD,
+                           "l2": "flushed between steps; dataset 512 MB > L2",
+                           "parallelism": "replicas x%d" % world},
+                "recall@10": ladder[P_star], "recall_ladder": ladder, "recall@100_at_P": recall100,
+                "build": {"seconds": build_ms / 1000, "wall_s": build_wall, "info": info},
+                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(Qh.nbytes),
+                        "d2h_bytes_per_step": int(hi.nbytes + hd.nbytes + hc.nbytes)},
+                "gpu_launches": args.steps,
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                             "frac": achieved / hbm, "traffic": None,
+                             "algorithmic_bytes_per_launch": int(bytes_per_launch)},
+                "clocks": clk.summary(), "cpu_baseline": cpu}
+        print(json.dumps(line))
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def ctx_save(path, off, ids, dists, M):
+    """Writes a CSR graph in the reference's index format (kgraph.cpp:349-372)."""
+    n = len(M)
+    off = off.astype(np.int64)
+    deg = np.diff(off)
+    words = np.zeros(5 + 2 * n + 3 * int(off[-1]), np.uint32)
+    words[:5] = np.frombuffer(b"KNNGRAPH", np.uint32).tolist() + [2, 0, n]
+    head = 5 + 2 * np.arange(n, dtype=np.int64) + 3 * off[:-1]
+    words[head] = M
+    words[head + 1] = deg
+    rec = np.repeat(head + 2 - 3 * off[:-1], deg) + 3 * np.arange(int(off[-1]), dtype=np.int64)
+    words[rec] = ids
+    words[rec + 1] = np.ascontiguousarray(dists, np.float32).view(np.uint32)
+    words.tofile(path)
+
+
+if __name__ == "__main__":
+    main()

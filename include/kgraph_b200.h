@@ -113,6 +113,9 @@ int kg_prune(kg_ctx *ctx, unsigned level);
 /* Milliseconds of the last kg_build / kg_search_batch device work, measured
  * with CUDA events on the context's stream (for profiling and benchmarks). */
 int kg_last_timing(kg_ctx *ctx, float *build_ms, float *search_ms);
+/* Work of the last kg_search_batch: distance evaluations (seeds included;
+ * the sum of SearchInfo.cost * N plus the seeds) and adjacency entries read. */
+int kg_last_search_work(kg_ctx *ctx, uint64_t *evaluations, uint64_t *adjacency_reads);
 
 #ifdef __cplusplus
 }

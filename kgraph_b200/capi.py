@@ -19,6 +19,7 @@ SYMBOLS = [
     "kg_index_params_default", "kg_search_params_default", "kg_ctx_create", "kg_ctx_destroy",
     "kg_last_error", "kg_version", "kg_set_verbosity", "kg_set_data", "kg_build", "kg_graph_size",
     "kg_graph_export", "kg_graph_import", "kg_search_batch", "kg_reverse", "kg_prune", "kg_last_timing",
+    "kg_last_search_work",
 ]
 
 
@@ -64,6 +65,7 @@ def lib():
         L.kg_reverse.argtypes = [vp, C.c_int]
         L.kg_prune.argtypes = [vp, C.c_uint]
         L.kg_last_timing.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.kg_last_search_work.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
         L.kg_index_params_default.argtypes = [C.POINTER(IndexParams)]
         L.kg_search_params_default.argtypes = [C.POINTER(SearchParams)]
         _lib = L
@@ -179,6 +181,11 @@ class Context:
 
     def prune(self, level):
         self._check(self.L.kg_prune(self.h, level))
+
+    def search_work(self):
+        ev, adj = C.c_uint64(), C.c_uint64()
+        self._check(self.L.kg_last_search_work(self.h, C.byref(ev), C.byref(adj)))
+        return ev.value, adj.value
 
     def timing(self):
         b, s = C.c_float(), C.c_float()

@@ -1,27 +1,719 @@
-// NN-descent construction on the GPU (KGraphConstructor, kgraph.cpp:705-1001).
+// NN-descent construction on the GPU: KGraphConstructor (kgraph.cpp:705-1001).
+//
+// Per node the state lives in HBM as structure-of-arrays rows (kg_build.h).
+// One iteration is the reference's  join -> statistics -> stop test -> update:
+//
+//   join_kernel      one warp per node: every new x new pair (i < j by id) and
+//                    new x old pair, canonical FP32 distance by 4-lane groups
+//                    (8 pairs per pass), then Nhood::parallel_try_insert into
+//                    both pools: unlocked radius test, per-node lock, the
+//                    warp's sorted insert with the reference's duplicate and
+//                    overflow-slot rules (kgraph.cpp:723-736, 797-815).
+//   stats kernels    delta, mean M, control recall/accuracy (kgraph.cpp:927-963).
+//   update kernels   radius = pool[L], M growth, radiusM, new/old split with
+//                    flag clearing, reverse samples by the radiusM rule in an
+//                    exact count-scan-fill CSR, then a uniform R-subset per
+//                    node (kgraph.cpp:816-883).
+//
+// Randomness.  The reference's init draws from one mt19937 per OpenMP thread
+// and its R cap from the C library rand(), so its graph depends on thread
+// count and scheduling.  Here each node draws from its own SplitMix64 stream
+// keyed by (seed, node, purpose): same GenRandom algorithm and distribution,
+// independent of launch shape.
+#include <cub/cub.cuh>
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <iostream>
+#include <numeric>
+#include <random>
+#include "kg_build.h"
 #include "kg_ctx.h"
+#include "kg_sort.h"
+#include "kg_warp.cuh"
+
+namespace kgb {
+
+unsigned g_verbosity = 1;
+
+namespace {
+
+constexpr long long LOCK_LIMIT_CYCLES = 4000000000ll;   // ~2 s at 2 GHz, then an error is reported
+
+// SplitMix64 (Steele, Lea, Flood 2014): one stream per (seed, node, purpose).
+struct Rng {
+    uint64_t s;
+    __device__ uint32_t next() {
+        s += 0x9E3779B97F4A7C15ull;
+        uint64_t z = s;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return (uint32_t)((z ^ (z >> 31)) >> 32);
+    }
+};
+__device__ Rng make_rng(uint64_t seed, uint64_t node, uint64_t purpose) {
+    Rng r{seed ^ (node * 0xD1B54A32D192ED03ull) ^ (purpose << 56)};
+    r.next();
+    r.next();
+    return r;
+}
+
+// GenRandom (kgraph.cpp:44-65) by one thread, in place in global memory.
+__device__ void gen_random_dev(Rng &rng, uint32_t *addr, uint32_t size, uint32_t N) {
+    if (N == size) {
+        for (uint32_t i = 0; i < size; ++i) addr[i] = i;
+        return;
+    }
+    for (uint32_t i = 0; i < size; ++i) addr[i] = rng.next() % (N - size);
+    for (uint32_t i = 1; i < size; ++i) {   // insertion sort (size is 2S or S+1)
+        uint32_t v = addr[i];
+        uint32_t j = i;
+        while (j > 0 && addr[j - 1] > v) { addr[j] = addr[j - 1]; --j; }
+        addr[j] = v;
+    }
+    for (uint32_t i = 1; i < size; ++i)
+        if (addr[i] <= addr[i - 1]) addr[i] = addr[i - 1] + 1;
+    uint32_t off = rng.next() % N;
+    for (uint32_t i = 0; i < size; ++i) addr[i] = (addr[i] + off) % N;
+}
+
+struct GPoolAcc {   // gnu_sort over one pool row (dist, id) in global memory
+    float *d; uint32_t *i;
+    struct Rec { float d; uint32_t i; };
+    __device__ float key(int x) const { return d[x]; }
+    __device__ void swap(int x, int y) const {
+        float td = d[x]; d[x] = d[y]; d[y] = td;
+        uint32_t ti = i[x]; i[x] = i[y]; i[y] = ti;
+    }
+    __device__ Rec get(int x) const { return Rec{d[x], i[x]}; }
+    __device__ void put(int x, Rec r) const { d[x] = r.d; i[x] = r.i; }
+    __device__ float rkey(Rec r) const { return r.d; }
+};
+
+__device__ __forceinline__ uint32_t warp_id_global() { return (blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
+__device__ __forceinline__ uint32_t warps_total() { return (gridDim.x * blockDim.x) >> 5; }
+
+// ------------------------------------------------------------------ init
+// kgraph.cpp:760-796 for one node per warp.
+__global__ void __launch_bounds__(256) init_kernel(BuildState s) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t N = s.D.n;
+    for (uint32_t n = warp_id_global(); n < N; n += warps_total()) {
+        uint32_t *pi = s.pool_i + (size_t)n * s.PS;
+        float *pd = s.pool_d + (size_t)n * s.PS;
+        if (lane == 0) {
+            Rng rng = make_rng(s.seed, n, 1);
+            gen_random_dev(rng, s.nn_new + (size_t)n * s.NEWCAP, 2 * s.S, N);
+            gen_random_dev(rng, pi, s.S + 1, N);        // `random`, consumed in place below
+            uint32_t i = 0;
+            for (uint32_t l = 0; l < s.S; ++l) {
+                if (pi[i] == n) ++i;
+                pi[l] = pi[i++];
+            }
+        }
+        __syncwarp();
+        const int g = lane >> 2, t = lane & 3;
+        for (uint32_t base = 0; base < s.S; base += 8) {
+            uint32_t l = base + g;
+            uint32_t id = l < s.S ? pi[l] : n;
+            float dd = pair_dist(s.D, id, n, t, FULL);
+            __syncwarp();
+            if (l < s.S && t == 0) { pd[l] = dd; pi[l] = id | FLAG_BIT; }
+        }
+        for (uint32_t l = s.S + lane; l < s.PS; l += 32) { pd[l] = FLT_MAX; pi[l] = UNSET_ID; }
+        __syncwarp();
+        if (lane == 0) {
+            GPoolAcc acc{pd, pi};
+            gnu_sort(acc, 0, (int)s.S);   // kgraph.cpp:793
+            s.nodeL[n] = s.S;
+            s.nodeM[n] = s.S;
+            s.radius[n] = FLT_MAX;
+            s.cnt_new[n] = 2 * s.S;
+            s.cnt_old[n] = 0;
+            s.found[n] = 0;
+            s.lock[n] = 0;
+        }
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------------------------ join
+// Nhood::parallel_try_insert (kgraph.cpp:723-736) by one warp.  Returns the
+// reference's value: pool.size() when the radius test rejects, L+1 for a
+// duplicate, else the insert position.
+__device__ uint32_t locked_insert(const BuildState &s, uint32_t x, uint32_t y, float d, int lane) {
+    float rad = *reinterpret_cast<volatile float *>(s.radius + x);
+    if (d > rad) return s.Lp;
+    uint32_t ok = 1;
+    if (lane == 0) {
+        long long t0 = clock64();
+        while (atomicCAS(s.lock + x, 0u, 1u) != 0u) {
+            if (clock64() - t0 > LOCK_LIMIT_CYCLES) { ok = 0; raise_error(s.err, ERR_LOCK_TIMEOUT); break; }
+            __nanosleep(32);
+        }
+    }
+    ok = __shfl_sync(FULL, ok, 0);
+    if (!ok) return s.Lp;
+    __threadfence();
+    volatile float *pd = s.pool_d + (size_t)x * s.PS;
+    volatile uint32_t *pi = s.pool_i + (size_t)x * s.PS;
+    const uint32_t Lc = *reinterpret_cast<volatile uint32_t *>(s.nodeL + x);
+    uint32_t r = warp_update_knn(pd, pi, (uint32_t *)nullptr, Lc, d, y | FLAG_BIT, 0u, lane);
+    if (r <= Lc) {
+        if (Lc + 1 < s.Lp) {
+            if (lane == 0) *reinterpret_cast<volatile uint32_t *>(s.nodeL + x) = Lc + 1;
+        } else {
+            float nr = pd[Lc - 1];
+            if (lane == 0) *reinterpret_cast<volatile float *>(s.radius + x) = nr;
+        }
+    }
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) atomicExch(s.lock + x, 0u);
+    return r;
+}
+
+// KGraphConstructor::join + Nhood::join (kgraph.cpp:740-751, 797-815).
+__global__ void __launch_bounds__(256) join_kernel(BuildState s) {
+    const int lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const uint32_t N = s.D.n;
+    unsigned long long comps = 0;
+    for (;;) {
+        uint32_t n = 0;
+        if (lane == 0) n = atomicAdd(s.work, 1u);
+        n = __shfl_sync(FULL, n, 0);
+        if (n >= N) break;
+        const uint32_t a = s.cnt_new[n], b = s.cnt_old[n];
+        const uint32_t *nw = s.nn_new + (size_t)n * s.NEWCAP;
+        const uint32_t *od = s.nn_old + (size_t)n * s.OLDCAP;
+        bool uu = false;
+        for (uint32_t ii = 0; ii < a; ++ii) {
+            const uint32_t iid = nw[ii];
+            const uint32_t nnn = a - ii - 1, inner = nnn + b;
+            for (uint32_t base = 0; base < inner; base += 8) {
+                const uint32_t k = base + g;
+                bool valid = k < inner;
+                const bool is_nn = k < nnn;
+                uint32_t jid = valid ? (is_nn ? nw[ii + 1 + k] : od[k - nnn]) : 0u;
+                if (valid && is_nn && jid == iid) valid = false;   // i < j by id excludes equal ids
+                uint32_t x = valid ? (is_nn ? min(iid, jid) : iid) : 0u;
+                uint32_t y = valid ? (is_nn ? max(iid, jid) : jid) : 0u;
+                if (valid && (x >= N || y >= N)) { raise_error(s.err, ERR_BAD_ID); valid = false; x = y = 0; }
+                float dd = pair_dist(s.D, x, y, t, FULL);
+                // parallel unlocked radius pre-test for both directions
+                float rx = (valid && t == 0) ? *reinterpret_cast<volatile float *>(s.radius + x) : 0.f;
+                float ry = (valid && t == 1) ? *reinterpret_cast<volatile float *>(s.radius + y) : 0.f;
+                unsigned vm = __ballot_sync(FULL, valid && t == 0);
+                unsigned nx = __ballot_sync(FULL, valid && t == 0 && !(dd > rx));
+                unsigned ny = __ballot_sync(FULL, valid && t == 1 && !(dd > ry));
+                comps += __popc(vm);
+                while (vm) {
+                    const int src = __ffs(vm) - 1;
+                    vm &= vm - 1;
+                    const uint32_t xg = __shfl_sync(FULL, x, src), yg = __shfl_sync(FULL, y, src);
+                    const float dg = __shfl_sync(FULL, dd, src);
+                    uint32_t r = s.Lp;
+                    if (nx & (1u << src)) r = locked_insert(s, xg, yg, dg, lane);
+                    if (r < s.K) uu = true;
+                    if (ny & (1u << (src + 1))) locked_insert(s, yg, xg, dg, lane);
+                }
+            }
+        }
+        if (lane == 0) s.found[n] = uu ? 1u : 0u;
+    }
+    if (lane == 0 && comps) atomicAdd(s.n_comps, comps);
+}
+
+// ------------------------------------------------------------------ statistics
+// Flags in pool[0..K) (EvaluateDelta, kgraph.cpp:148-156) and the sum of M.
+__global__ void stats_kernel(BuildState s) {
+    unsigned long long fl = 0, msum = 0;
+    const uint32_t lim = min(s.K, s.Lp);
+    for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < s.D.n; n += gridDim.x * blockDim.x) {
+        const uint32_t *pi = s.pool_i + (size_t)n * s.PS;
+        for (uint32_t l = 0; l < lim; ++l) fl += (pi[l] & FLAG_BIT) ? 1 : 0;
+        msum += s.nodeM[n];
+    }
+    for (int o = 16; o; o >>= 1) {
+        fl += __shfl_xor_sync(FULL, fl, o);
+        msum += __shfl_xor_sync(FULL, msum, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(s.stat + 0, fl);
+        atomicAdd(s.stat + 1, msum);
+    }
+}
+
+// Control nodes: EvaluateRecall / EvaluateAccuracy / EvaluateOneRecall
+// (kgraph.cpp:96-146) against their exact K-NN.  out[c*5 + ...] = recall,
+// accuracy, one-recall, pool[0].dist, exact[0].dist; recall < 0 marks the
+// reference's "distance is unstable" failure.
+__global__ void controls_kernel(BuildState s, const uint32_t *ctrl, const float *exact_d, uint32_t C, float *out) {
+    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C) return;
+    const uint32_t node = ctrl[c];
+    const float *pd = s.pool_d + (size_t)node * s.PS;
+    const float *kd = exact_d + (size_t)c * s.K;
+    const uint32_t P = s.Lp, K = s.K;
+    float recall;
+    if (K == 0) recall = 1.0f;
+    else {
+        uint32_t found = 0, np = 0, nk = 0;
+        bool bad = false;
+        while (np < P && nk < K) {
+            if (kd[nk] < pd[np]) ++nk;
+            else if (kd[nk] == pd[np]) { ++found; ++nk; ++np; }
+            else { bad = true; break; }
+        }
+        recall = bad ? -1.0f : __fdiv_rn((float)found, (float)K);
+    }
+    uint32_t m = min(P, K), cnt = 0;
+    float sum = 0.f;
+    for (uint32_t i = 0; i < m; ++i)
+        if (kd[i] > 0) { sum = __fadd_rn(sum, __fdiv_rn(fabsf(__fsub_rn(pd[i], kd[i])), kd[i])); ++cnt; }
+    out[c * 5 + 0] = recall;
+    out[c * 5 + 1] = cnt > 0 ? __fdiv_rn(sum, (float)cnt) : 0.f;
+    out[c * 5 + 2] = (K > 0 && pd[0] == kd[0]) ? 1.f : 0.f;
+    out[c * 5 + 3] = pd[0];
+    out[c * 5 + 4] = K > 0 ? kd[0] : 0.f;
+}
+
+// ------------------------------------------------------------------ update
+// kgraph.cpp:818-841: radius, M growth, radiusM; clears the per-node lists.
+__global__ void update_m_kernel(BuildState s) {
+    for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < s.D.n; n += gridDim.x * blockDim.x) {
+        const float *pd = s.pool_d + (size_t)n * s.PS;
+        const uint32_t *pi = s.pool_i + (size_t)n * s.PS;
+        s.radius[n] = pd[s.L];   // pool.back()
+        uint32_t M = s.nodeM[n];
+        if (s.found[n]) {
+            uint32_t maxl = min(M + s.S, s.nodeL[n]);
+            uint32_t c = 0, l = 0;
+            while (l < maxl && c < s.S) {
+                if (pi[l] & FLAG_BIT) ++c;
+                ++l;
+            }
+            M = l;
+            s.nodeM[n] = M;
+        }
+        if (M == 0) { raise_error(s.err, ERR_CAPACITY); M = 1; }
+        s.radiusM[n] = pd[M - 1];
+        s.rcnt_new[n] = 0;
+        s.rcnt_old[n] = 0;
+    }
+}
+
+// Counts the reverse samples each node will receive (kgraph.cpp:852, 860).
+__global__ void update_count_kernel(BuildState s) {
+    const int lane = threadIdx.x & 31;
+    for (uint32_t n = warp_id_global(); n < s.D.n; n += warps_total()) {
+        const float *pd = s.pool_d + (size_t)n * s.PS;
+        const uint32_t *pi = s.pool_i + (size_t)n * s.PS;
+        const uint32_t M = s.nodeM[n];
+        for (uint32_t l = lane; l < M; l += 32) {
+            uint32_t e = pi[l], id = e & ID_MASK;
+            if (id >= s.D.n) { raise_error(s.err, ERR_BAD_ID); continue; }
+            if (pd[l] > s.radiusM[id]) atomicAdd((e & FLAG_BIT) ? s.rcnt_new + id : s.rcnt_old + id, 1u);
+        }
+    }
+}
+
+// kgraph.cpp:842-866: forward new/old lists in pool order, flags cleared on
+// the new ones, reverse samples appended to their targets' CSR buckets.
+__global__ void update_fill_kernel(BuildState s) {
+    const int lane = threadIdx.x & 31;
+    for (uint32_t n = warp_id_global(); n < s.D.n; n += warps_total()) {
+        float *pd = s.pool_d + (size_t)n * s.PS;
+        uint32_t *pi = s.pool_i + (size_t)n * s.PS;
+        uint32_t *nw = s.nn_new + (size_t)n * s.NEWCAP;
+        uint32_t *od = s.nn_old + (size_t)n * s.OLDCAP;
+        const uint32_t M = s.nodeM[n];
+        uint32_t cn = 0, co = 0;
+        for (uint32_t base = 0; base < M; base += 32) {
+            const uint32_t l = base + lane;
+            const bool act = l < M;
+            uint32_t e = act ? pi[l] : 0u, id = e & ID_MASK;
+            const bool fl = act && (e & FLAG_BIT);
+            const bool ok = act && id < s.D.n;
+            unsigned mn = __ballot_sync(FULL, fl), mo = __ballot_sync(FULL, act && !fl);
+            unsigned below = (1u << lane) - 1u;
+            if (fl) { nw[cn + __popc(mn & below)] = id; pi[l] = id; }
+            if (act && !fl) od[co + __popc(mo & below)] = id;
+            if (ok && pd[l] > s.radiusM[id]) {
+                if (fl) {
+                    uint32_t p = atomicAdd(s.rcnt_new + id, 1u);
+                    s.rbuf_new[s.roff_new[id] + p] = n;
+                } else {
+                    uint32_t p = atomicAdd(s.rcnt_old + id, 1u);
+                    s.rbuf_old[s.roff_old[id] + p] = n;
+                }
+            }
+            cn += __popc(mn);
+            co += __popc(mo);
+        }
+        if (lane == 0) { s.cnt_new[n] = cn; s.cnt_old[n] = co; }
+    }
+}
+
+// kgraph.cpp:867-882: at most R reverse samples, a uniform random subset, appended.
+__global__ void update_cap_kernel(BuildState s) {
+    const int lane = threadIdx.x & 31;
+    for (uint32_t n = warp_id_global(); n < s.D.n; n += warps_total()) {
+        for (int kind = 0; kind < 2; ++kind) {
+            uint32_t *src = kind == 0 ? s.rbuf_new + s.roff_new[n] : s.rbuf_old + s.roff_old[n];
+            const uint32_t c = (uint32_t)((kind == 0 ? s.roff_new[n + 1] : s.roff_old[n + 1]) -
+                                          (kind == 0 ? s.roff_new[n] : s.roff_old[n]));
+            uint32_t take = c;
+            if (s.R && c > s.R) {
+                take = s.R;
+                if (lane == 0) {   // partial Fisher-Yates: the first R of a uniform shuffle
+                    Rng rng = make_rng(s.seed, n, 16 + 2 * (uint64_t)s.iteration + kind);
+                    for (uint32_t i = 0; i < take; ++i) {
+                        uint32_t j = i + rng.next() % (c - i);
+                        uint32_t tmp = src[i]; src[i] = src[j]; src[j] = tmp;
+                    }
+                }
+                __syncwarp();
+            }
+            uint32_t *dst = kind == 0 ? s.nn_new + (size_t)n * s.NEWCAP : s.nn_old + (size_t)n * s.OLDCAP;
+            uint32_t *cnt = kind == 0 ? s.cnt_new + n : s.cnt_old + n;
+            const uint32_t cap = kind == 0 ? s.NEWCAP : s.OLDCAP;
+            const uint32_t have = *cnt;
+            if (have + take > cap) {
+                if (lane == 0) raise_error(s.err, ERR_CAPACITY);
+                take = cap > have ? cap - have : 0;
+            }
+            for (uint32_t i = lane; i < take; i += 32) dst[have + i] = src[i];
+            __syncwarp();
+            if (lane == 0) *cnt = have + take;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ finalize
+__global__ void finalize_count_kernel(BuildState s, uint64_t *cnt) {
+    for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < s.D.n; n += gridDim.x * blockDim.x)
+        cnt[n] = min(s.L, s.nodeL[n]);
+}
+__global__ void finalize_fill_kernel(BuildState s, const uint64_t *off, uint32_t *ids, float *dists, uint32_t *M) {
+    const int lane = threadIdx.x & 31;
+    for (uint32_t n = warp_id_global(); n < s.D.n; n += warps_total()) {
+        const uint64_t o = off[n];
+        const uint32_t c = (uint32_t)(off[n + 1] - o);
+        for (uint32_t l = lane; l < c; l += 32) {
+            ids[o + l] = s.pool_i[(size_t)n * s.PS + l] & ID_MASK;
+            dists[o + l] = s.pool_d[(size_t)n * s.PS + l];
+        }
+        if (lane == 0) M[n] = s.nodeM[n];
+    }
+}
+
+// ------------------------------------------------------------------ controls' exact K-NN
+// LinearSearch (kgraph.cpp:212-229): rows [lo, hi) of the scan for control c
+// by one warp, keeping the K best by (distance, id) -- the order the
+// reference's in-id-order insert-after-equals produces.
+__global__ void __launch_bounds__(256) linear_part_kernel(DataView D, const uint32_t *ctrl, uint32_t C, uint32_t K,
+                                                          uint32_t parts, float *part_d, uint32_t *part_i,
+                                                          uint32_t *part_n) {
+    extern __shared__ __align__(16) char smem[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const uint32_t w = warp_id_global();
+    if (w >= C * parts) return;   // whole warps exit together
+    const uint32_t c = w / parts, part = w % parts;
+    const uint32_t self = ctrl[c];
+    const uint32_t chunk = (D.n + parts - 1) / parts;
+    const uint32_t lo = part * chunk, hi = min(D.n, lo + chunk);
+    float *ld = reinterpret_cast<float *>(smem) + (size_t)wib * (2 * (K + 1) + 16);
+    uint32_t *li = reinterpret_cast<uint32_t *>(ld + (K + 1));
+    float *cd = ld + 2 * (K + 1);
+    uint32_t L = 0;
+    for (uint32_t base = lo; base < hi; base += 8) {
+        uint32_t row = base + g;
+        bool v = row < hi && row != self;
+        float dd = pair_dist(D, self, v ? row : self, t, FULL);
+        if (t == 0) cd[g] = dd;
+        __syncwarp();
+        unsigned vm = __ballot_sync(FULL, v && t == 0);
+        while (vm) {
+            int src = __ffs(vm) - 1;
+            vm &= vm - 1;
+            float x = cd[src >> 2];
+            if (L == K && (K == 0 || x >= ld[K - 1])) continue;
+            warp_update_knn(ld, li, (uint32_t *)nullptr, L, x, base + (src >> 2), 0u, lane);
+            if (L < K) ++L;
+        }
+        __syncwarp();
+    }
+    float *od = part_d + (size_t)w * K;
+    uint32_t *oi = part_i + (size_t)w * K;
+    for (uint32_t k = lane; k < L; k += 32) { od[k] = ld[k]; oi[k] = li[k]; }
+    if (lane == 0) part_n[w] = L;
+}
+
+// Merges the parts of each control in part order (= id order), keeping K.
+__global__ void __launch_bounds__(256) linear_merge_kernel(uint32_t C, uint32_t K, uint32_t parts, const float *part_d,
+                                                           const uint32_t *part_i, const uint32_t *part_n, float *out_d,
+                                                           uint32_t *out_i) {
+    extern __shared__ __align__(16) char smem[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const uint32_t c = warp_id_global();
+    if (c >= C) return;
+    float *ld = reinterpret_cast<float *>(smem) + (size_t)wib * 2 * (K + 1);
+    uint32_t *li = reinterpret_cast<uint32_t *>(ld + (K + 1));
+    uint32_t L = 0;
+    for (uint32_t p = 0; p < parts; ++p) {
+        const uint32_t w = c * parts + p;
+        for (uint32_t k = 0; k < part_n[w]; ++k) {
+            float x = part_d[(size_t)w * K + k];
+            if (L == K && (K == 0 || x >= ld[K - 1])) break;   // parts are sorted: the rest cannot enter
+            warp_update_knn(ld, li, (uint32_t *)nullptr, L, x, part_i[(size_t)w * K + k], 0u, lane);
+            if (L < K) ++L;
+        }
+    }
+    for (uint32_t k = lane; k < K; k += 32) {
+        out_d[(size_t)c * K + k] = k < L ? ld[k] : FLT_MAX;
+        out_i[(size_t)c * K + k] = k < L ? li[k] : UNSET_ID;
+    }
+}
+
+int grid_for(kg_ctx *ctx, int per_sm = 8) { return ctx->num_sms * per_sm; }
+
+}  // namespace
+
+// Exact K-NN of control rows (GenerateControl, kgraph.cpp:254-270).
+cudaError_t launch_linear_search(kg_ctx *ctx, const uint32_t *rows, uint32_t C, uint32_t K, uint32_t *out_i,
+                                 float *out_d) {
+    DataView D{ctx->X.as<float>(), ctx->norms.as<float>(), ctx->n, ctx->d, ctx->ld, ctx->metric};
+    uint32_t parts = std::max<uint32_t>(1, std::min<uint32_t>(ctx->n / 2048 + 1, (uint32_t)(ctx->num_sms * 64 / std::max(C, 1u))));
+    size_t nw = (size_t)C * parts;
+    DevBuf &pd = ctx->build_scratch[20], &pi = ctx->build_scratch[21], &pn = ctx->build_scratch[22];
+    cudaError_t e;
+    if ((e = pd.reserve(nw * K * 4 + 4)) != cudaSuccess || (e = pi.reserve(nw * K * 4 + 4)) != cudaSuccess ||
+        (e = pn.reserve(nw * 4 + 4)) != cudaSuccess)
+        return e;
+    size_t smem1 = 8 * ((2 * (K + 1) + 16) * 4);
+    size_t smem2 = 8 * (2 * (K + 1) * 4);
+    if (smem1 > 48 * 1024) cudaFuncSetAttribute(linear_part_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1);
+    if (smem2 > 48 * 1024) cudaFuncSetAttribute(linear_merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2);
+    linear_part_kernel<<<(unsigned)((nw + 7) / 8), 256, smem1, ctx->stream>>>(D, rows, C, K, parts, pd.as<float>(),
+                                                                                 pi.as<uint32_t>(), pn.as<uint32_t>());
+    linear_merge_kernel<<<(C + 7) / 8, 256, smem2, ctx->stream>>>(C, K, parts, pd.as<float>(), pi.as<uint32_t>(),
+                                                                   pn.as<uint32_t>(), out_d, out_i);
+    return cudaGetLastError();
+}
+
+// Exclusive scan of n u32/u64 counts into out[n+1] (CUB).
+cudaError_t scan_counts(kg_ctx *ctx, const uint32_t *in, uint64_t *out, uint32_t n) {
+    DevBuf &tmp = ctx->build_scratch[23];
+    size_t bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n + 1, ctx->stream);
+    cudaError_t e = tmp.reserve(bytes);
+    if (e != cudaSuccess) return e;
+    return cub::DeviceScan::ExclusiveSum(tmp.p, bytes, in, out, n + 1, ctx->stream);
+}
+cudaError_t scan_counts64(kg_ctx *ctx, const uint64_t *in, uint64_t *out, uint32_t n) {
+    DevBuf &tmp = ctx->build_scratch[23];
+    size_t bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n + 1, ctx->stream);
+    cudaError_t e = tmp.reserve(bytes);
+    if (e != cudaSuccess) return e;
+    return cub::DeviceScan::ExclusiveSum(tmp.p, bytes, in, out, n + 1, ctx->stream);
+}
+
+}  // namespace kgb
 
 using namespace kgb;
 
-static unsigned g_verbosity = 1;
+extern "C" void kg_set_verbosity(unsigned v) { kgb::g_verbosity = v; }
 
-extern "C" {
-
-void kg_set_verbosity(unsigned v) { g_verbosity = v; }
-
-int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_info *info) {
-    (void)params; (void)info;
-    return set_error(ctx, KG_E_RUNTIME, "build not available yet");
+// Implemented in kg_graph.cu.
+namespace kgb {
+int graph_reverse(kg_ctx *ctx, int rev_k);
+int graph_prune(kg_ctx *ctx, unsigned level);
 }
 
-int kg_reverse(kg_ctx *ctx, int rev_k) {
-    (void)rev_k;
-    return set_error(ctx, KG_E_RUNTIME, "reverse not available yet");
-}
+extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_info *info) {
+    if (!ctx) return KG_E_INVALID;
+    std::lock_guard<std::mutex> guard(ctx->mu);
+    cudaSetDevice(ctx->device);
+    if (!ctx->has_data) return set_error(ctx, KG_E_RUNTIME, "no dataset");
+    if (!params) return set_error(ctx, KG_E_INVALID, "bad arguments");
+    auto t_start = std::chrono::steady_clock::now();
+    const uint32_t N = ctx->n;
+    uint32_t L = params->L, K = params->K, S = params->S, C = params->controls;
+    // kgraph.cpp:893-905
+    if (N <= K) return set_error(ctx, KG_E_RUNTIME, "K larger than dataset size");
+    if (N < C) {
+        std::cerr << "Warning: small dataset, shrinking control size to " << N << "." << std::endl;
+        C = N;
+    }
+    if (N <= L) {
+        std::cerr << "Warning: small dataset, shrinking L to " << (N - 1) << "." << std::endl;
+        L = N - 1;
+    }
+    if (N <= S) {
+        std::cerr << "Warning: small dataset, shrinking S to " << (N - 1) << "." << std::endl;
+        S = N - 1;
+    }
+    if (S == 0 || S > L) return set_error(ctx, KG_E_INVALID, "S must be in [1, L]");
+    if (params->prune > 2) return set_error(ctx, KG_E_RUNTIME, "prune level not supported.");
 
-int kg_prune(kg_ctx *ctx, unsigned level) {
-    (void)level;
-    return set_error(ctx, KG_E_RUNTIME, "prune not available yet");
-}
+    BuildState s{};
+    s.D = DataView{ctx->X.as<float>(), ctx->norms.as<float>(), N, ctx->d, ctx->ld, ctx->metric};
+    s.L = L; s.Lp = L + 1; s.K = K; s.S = S; s.R = params->R;
+    s.PS = (s.Lp + 7) / 8 * 8;
+    s.NEWCAP = std::max(2 * S, L) + s.R;
+    s.OLDCAP = L + s.R;
+    s.seed = ((uint64_t)params->seed << 32) ^ 0x5851F42D4C957F2Dull;
 
+    DevBuf *B = ctx->build_scratch;
+    const size_t n = N;
+    cudaError_t e;
+    size_t need[] = {n * s.PS * 4, n * s.PS * 4, n * 4, n * 4, n * 4, n * 4, n * 4, n * 4,
+                     n * s.NEWCAP * 4, n * 4, n * s.OLDCAP * 4, n * 4, (n + 1) * 4, (n + 1) * 4,
+                     (n + 1) * 8, (n + 1) * 8, n * L * 4 + 4, n * L * 4 + 4, 64};
+    for (int i = 0; i < 19; ++i)
+        if ((e = B[i].reserve(need[i])) != cudaSuccess) return cuda_fail(ctx, e, "alloc build state");
+    s.pool_d = B[0].as<float>(); s.pool_i = B[1].as<uint32_t>();
+    s.nodeL = B[2].as<uint32_t>(); s.nodeM = B[3].as<uint32_t>();
+    s.radius = B[4].as<float>(); s.radiusM = B[5].as<float>();
+    s.found = B[6].as<uint32_t>(); s.lock = B[7].as<uint32_t>();
+    s.nn_new = B[8].as<uint32_t>(); s.cnt_new = B[9].as<uint32_t>();
+    s.nn_old = B[10].as<uint32_t>(); s.cnt_old = B[11].as<uint32_t>();
+    s.rcnt_new = B[12].as<uint32_t>(); s.rcnt_old = B[13].as<uint32_t>();
+    s.roff_new = B[14].as<uint64_t>(); s.roff_old = B[15].as<uint64_t>();
+    s.rbuf_new = B[16].as<uint32_t>(); s.rbuf_old = B[17].as<uint32_t>();
+    s.n_comps = B[18].as<unsigned long long>();
+    s.stat = s.n_comps + 1;
+    s.work = reinterpret_cast<uint32_t *>(s.n_comps + 4);
+    s.err = ctx->errw.as<uint32_t>();
+    cudaStream_t st = ctx->stream;
+    cudaMemsetAsync(B[18].p, 0, 64, st);
+    cudaMemsetAsync(s.rcnt_new + N, 0, 4, st);   // scan inputs carry one extra zero
+    cudaMemsetAsync(s.rcnt_old + N, 0, 4, st);
+
+    // GenerateControl (kgraph.cpp:254-270): C distinct random nodes, exact K-NN.
+    if (g_verbosity > 0) std::cerr << "Generating control..." << std::endl;
+    std::vector<uint32_t> hctrl(C);
+    {
+        std::mt19937 rng(params->seed);
+        std::vector<uint32_t> idx(N);
+        std::iota(idx.begin(), idx.end(), 0u);
+        for (uint32_t i = 0; i < C; ++i) {
+            uint32_t j = i + rng() % (N - i);
+            std::swap(idx[i], idx[j]);
+            hctrl[i] = idx[i];
+        }
+    }
+    DevBuf &dctrl = B[19];
+    if ((e = dctrl.reserve((size_t)C * 4 + (size_t)C * K * 8 + (size_t)C * 5 * 4 + 16)) != cudaSuccess)
+        return cuda_fail(ctx, e, "alloc controls");
+    uint32_t *ctrl = dctrl.as<uint32_t>();
+    uint32_t *ctrl_i = ctrl + C;
+    float *ctrl_d = reinterpret_cast<float *>(ctrl_i + (size_t)C * K);
+    float *ctrl_out = ctrl_d + (size_t)C * K;
+    cudaMemcpyAsync(ctrl, hctrl.data(), (size_t)C * 4, cudaMemcpyHostToDevice, st);
+    cudaEventRecord(ctx->ev0, st);
+    if (C && (e = launch_linear_search(ctx, ctrl, C, K, ctrl_i, ctrl_d)) != cudaSuccess)
+        return cuda_fail(ctx, e, "controls");
+
+    if (g_verbosity > 0) std::cerr << "Initializing..." << std::endl;
+    init_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "init");
+
+    kg_index_info inf{};
+    inf.stop_condition = 0;
+    inf.recall = 0;
+    inf.accuracy = std::numeric_limits<float>::max();
+    inf.cost = 0;
+    inf.iterations = 0;
+    inf.delta = 1.0f;
+    const float total = N * float(N - 1) / 2;
+    std::vector<float> hout((size_t)C * 5);
+    unsigned long long hstat[4];
+    for (uint32_t it = 0; (params->iterations <= 0) || (it < params->iterations); ++it) {
+        ++inf.iterations;
+        s.iteration = it;
+        cudaMemsetAsync(s.work, 0, 4, st);
+        join_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
+        cudaMemsetAsync(s.stat, 0, 16, st);
+        stats_kernel<<<grid_for(ctx, 4), 256, 0, st>>>(s);
+        if (C) controls_kernel<<<(C + 127) / 128, 128, 0, st>>>(s, ctrl, ctrl_d, C, ctrl_out);
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "join");
+        cudaMemcpyAsync(hstat, s.n_comps, 3 * 8, cudaMemcpyDeviceToHost, st);
+        if (C) cudaMemcpyAsync(hout.data(), ctrl_out, (size_t)C * 5 * 4, cudaMemcpyDeviceToHost, st);
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "join");
+        int de = check_device_error(ctx, "build");
+        if (de != KG_OK) return de;
+        // kgraph.cpp:927-963: the per-iteration statistics
+        inf.cost = hstat[0] / total;
+        inf.delta = (float)((double)hstat[1] / K / N);
+        inf.M = (float)((double)hstat[2] / N);
+        float rs = 0, as = 0, ors = 0, oa = 0, oe = 0;
+        for (uint32_t c = 0; c < C; ++c) {
+            if (hout[c * 5] < 0) return set_error(ctx, KG_E_RUNTIME, "distance is unstable");
+            rs += hout[c * 5]; as += hout[c * 5 + 1]; ors += hout[c * 5 + 2]; oa += hout[c * 5 + 3]; oe += hout[c * 5 + 4];
+        }
+        inf.recall = C ? rs / C : 0.f;
+        inf.accuracy = C ? as / C : 0.f;
+        if (g_verbosity > 0) {
+            auto now = std::chrono::steady_clock::now();
+            std::cerr << "iteration: " << inf.iterations << " recall: " << inf.recall << " accuracy: " << inf.accuracy
+                      << " cost: " << inf.cost << " M: " << inf.M << " delta: " << inf.delta
+                      << " time: " << std::chrono::duration<double>(now - t_start).count()
+                      << " one-recall: " << (C ? ors / C : 0.f) << " one-ratio: " << (C ? (oa / C) / (oe / C) : 0.f)
+                      << std::endl;
+        }
+        if (inf.delta <= params->delta) { inf.stop_condition = 1; break; }
+        if (inf.recall >= params->recall) { inf.stop_condition = 2; break; }
+        // update (kgraph.cpp:816-883)
+        update_m_kernel<<<grid_for(ctx, 4), 256, 0, st>>>(s);
+        update_count_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
+        if ((e = scan_counts(ctx, s.rcnt_new, s.roff_new, N)) != cudaSuccess) return cuda_fail(ctx, e, "scan");
+        if ((e = scan_counts(ctx, s.rcnt_old, s.roff_old, N)) != cudaSuccess) return cuda_fail(ctx, e, "scan");
+        cudaMemsetAsync(s.rcnt_new, 0, n * 4, st);
+        cudaMemsetAsync(s.rcnt_old, 0, n * 4, st);
+        update_fill_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
+        update_cap_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "update");
+    }
+
+    // finalize (kgraph.cpp:975-988) into the context's CSR graph
+    DevBuf &cnt = ctx->build_scratch[22];
+    if ((e = cnt.reserve((n + 1) * 8)) != cudaSuccess) return cuda_fail(ctx, e, "alloc");
+    cudaMemsetAsync(cnt.p, 0, (n + 1) * 8, st);
+    finalize_count_kernel<<<grid_for(ctx, 4), 256, 0, st>>>(s, cnt.as<uint64_t>());
+    if ((e = ctx->offsets.reserve((n + 1) * 8)) != cudaSuccess) return cuda_fail(ctx, e, "alloc graph");
+    if ((e = scan_counts64(ctx, cnt.as<uint64_t>(), ctx->offsets.as<uint64_t>(), N)) != cudaSuccess)
+        return cuda_fail(ctx, e, "scan");
+    uint64_t E = 0;
+    cudaMemcpyAsync(&E, ctx->offsets.as<uint64_t>() + N, 8, cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    if ((e = ctx->nbr.reserve(E * 4 + 4)) != cudaSuccess || (e = ctx->nbr_d.reserve(E * 4 + 4)) != cudaSuccess ||
+        (e = ctx->Mnode.reserve(n * 4)) != cudaSuccess)
+        return cuda_fail(ctx, e, "alloc graph");
+    finalize_fill_kernel<<<grid_for(ctx), 256, 0, st>>>(s, ctx->offsets.as<uint64_t>(), ctx->nbr.as<uint32_t>(),
+                                                         ctx->nbr_d.as<float>(), ctx->Mnode.as<uint32_t>());
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "finalize");
+    ctx->gn = N;
+    ctx->E = E;
+    ctx->no_dist = false;
+    ctx->has_graph = true;
+    int de = check_device_error(ctx, "build");
+    if (de != KG_OK) return de;
+    if (params->reverse) {
+        int r = graph_reverse(ctx, params->reverse);
+        if (r != KG_OK) return r;
+    }
+    if (params->prune) {
+        int r = graph_prune(ctx, params->prune);
+        if (r != KG_OK) return r;
+    }
+    cudaEventRecord(ctx->ev1, st);
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "build");
+    cudaEventElapsedTime(&ctx->last_build_ms, ctx->ev0, ctx->ev1);
+    if (info) *info = inf;
+    return KG_OK;
 }

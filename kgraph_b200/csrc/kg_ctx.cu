@@ -147,6 +147,13 @@ int kg_last_timing(kg_ctx *ctx, float *build_ms, float *search_ms) {
     return KG_OK;
 }
 
+int kg_last_search_work(kg_ctx *ctx, uint64_t *evaluations, uint64_t *adjacency_reads) {
+    if (!ctx) return KG_E_INVALID;
+    if (evaluations) *evaluations = ctx->last_work[0];
+    if (adjacency_reads) *adjacency_reads = ctx->last_work[1];
+    return KG_OK;
+}
+
 int kg_set_data(kg_ctx *ctx, const float *rows, size_t n, size_t d, size_t stride_bytes, int metric) {
     if (!ctx) return KG_E_INVALID;
     Lock lk(ctx);
@@ -381,7 +388,8 @@ int kg_search_batch(kg_ctx *ctx, const float *queries, size_t nq, size_t q_strid
     a.visited_slots = slots;
     a.qcounter = ctx->counter.as<uint32_t>();
     a.err = ctx->errw.as<uint32_t>();
-    cudaMemsetAsync(a.qcounter, 0, 4, ctx->stream);
+    a.work = reinterpret_cast<unsigned long long *>(ctx->counter.as<char>() + 16);
+    cudaMemsetAsync(ctx->counter.p, 0, 32, ctx->stream);
 
     cudaEventRecord(ctx->ev0, ctx->stream);
     if ((e = launch_search(a, ctx->num_sms, ctx->stream, nullptr)) != cudaSuccess) return cuda_fail(ctx, e, "search launch");
@@ -391,6 +399,7 @@ int kg_search_batch(kg_ctx *ctx, const float *queries, size_t nq, size_t q_strid
     if (dists && !d_dev) cudaMemcpyAsync(dists, a.out_dists, Q * out_ld * 4, cudaMemcpyDeviceToHost, ctx->stream);
     if (!c_dev) cudaMemcpyAsync(counts, a.out_count, Q * 4, cudaMemcpyDeviceToHost, ctx->stream);
     if (costs && !cost_dev) cudaMemcpyAsync(costs, a.out_cost, Q * 4, cudaMemcpyDeviceToHost, ctx->stream);
+    cudaMemcpyAsync(ctx->last_work, a.work, 16, cudaMemcpyDeviceToHost, ctx->stream);
     if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "search");
     cudaEventElapsedTime(&ctx->last_search_ms, ctx->ev0, ctx->ev1);
     return check_device_error(ctx, "search");

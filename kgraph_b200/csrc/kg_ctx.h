@@ -43,6 +43,7 @@ struct kg_ctx {
     std::mutex mu;
     std::string err;
     float last_build_ms = 0.f, last_search_ms = 0.f;
+    unsigned long long last_work[2] = {0, 0};
 
     // dataset
     kgb::DevBuf X, norms;

@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a) {
             *reinterpret_cast<uint4 *>(vis + w) = make_uint4(0u, 0u, 0u, 0u);
         __syncwarp();
 
-        uint32_t n_comps = 0;
+        uint32_t n_comps = 0, n_adj = 0, n_seed = 0;
         uint32_t rn = 0;          // results.size() - 1
         bool have_results = false;
         for (uint32_t trial = 0; trial < T; ++trial) {
@@ -194,6 +194,7 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a) {
                 for (uint32_t j = lane; j < L; j += 32) s.pid[j] = init[j];
             }
             __syncwarp();
+            n_seed += L;
             // kgraph.cpp:468-475: mark, flag, distance, m = 0, M = actual_M
             for (uint32_t base = 0; base < L; base += 32) {
                 uint32_t j = base + lane;
@@ -236,6 +237,7 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a) {
                 __syncwarp();
                 const uint32_t node = idf & ID_MASK;
                 const uint64_t nb = a.offsets[node];
+                n_adj += endM - beginM;
                 for (uint32_t m0 = beginM; m0 < endM; m0 += 32) {
                     const uint32_t cnt = min(32u, endM - m0);
                     bool act = lane < (int)cnt;
@@ -294,7 +296,14 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a) {
             if (out_d) out_d[k] = s.rd[k];
         }
         cost = __fdiv_rn((float)n_comps, (float)N);   // kgraph.cpp:561
-        if (lane == 0) { a.out_count[qi] = count; if (a.out_cost) a.out_cost[qi] = cost; }
+        if (lane == 0) {
+            a.out_count[qi] = count;
+            if (a.out_cost) a.out_cost[qi] = cost;
+            if (a.work) {
+                atomicAdd(a.work, (unsigned long long)(n_comps + n_seed));
+                atomicAdd(a.work + 1, (unsigned long long)n_adj);
+            }
+        }
         __syncwarp();
     }
 }

@@ -28,6 +28,7 @@ struct SearchArgs {
     uint32_t vwords, visited_slots;
     uint32_t *qcounter;         // zeroed before launch
     uint32_t *err;              // device error word
+    unsigned long long *work;   // [0] distance evaluations, [1] adjacency entries read (may be null)
     uint32_t cap, rcap;         // smem capacities: max(K+P+1), max(K+1)
     uint32_t warps_per_block, warp_smem_bytes;   // filled by launch_search
 };

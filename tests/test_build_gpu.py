@@ -1,0 +1,153 @@
+"""NN-descent build on the GPU, through the C-ABI.
+
+The reference's build is nondeterministic under OpenMP (per-thread RNG,
+racy inserts), so the graph is compared statistically: recall@K of the GPU
+graph against the exact K-NN must be within 0.005 of the reference's own
+build at the same parameters.  Everything deterministic is compared
+exactly: every stored distance is the canonical distance of its pair, lists
+are sorted and duplicate-free, reverse / prune of a given graph equal the
+reference's bit for bit.
+"""
+import numpy as np
+import pytest
+
+from conftest import load_golden
+from oracle import kgoracle as ko
+
+pytestmark = pytest.mark.gpu
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+def data(kind, n, d, seed):
+    rng = np.random.default_rng(seed)
+    if kind == "uniform":
+        return rng.random((n, d), dtype=np.float32)
+    if kind == "mixture":
+        c = rng.uniform(0, 128, (32, d))
+        x = c[rng.integers(0, 32, n)] + rng.normal(0, 20, (n, d))
+        return np.round(np.maximum(x, 0)).astype(np.float32)
+    x = rng.standard_normal((n, d)).astype(np.float32)
+    return x / np.linalg.norm(x, axis=1, keepdims=True)
+
+
+def exact_knn(ctx, X, K):
+    """Exact K-NN of every row, self excluded, through the GPU brute force."""
+    ids, d, cnt, _ = ctx.search(X, K=K + 1)
+    out_i = np.zeros((len(X), K), np.uint32)
+    out_d = np.zeros((len(X), K), np.float32)
+    for r in range(len(X)):
+        keep = ids[r] != r
+        out_i[r] = ids[r][keep][:K]
+        out_d[r] = d[r][keep][:K]
+    return out_i, out_d
+
+
+def graph_recall(G, ex_d, K):
+    """Mean over nodes of (#first-K graph entries with distance <= the exact K-th) / K: ties count."""
+    tot = 0
+    for r in range(G.n):
+        a, b = int(G.offsets[r]), int(G.offsets[r + 1])
+        dd = np.sort(G.dists[a:b])[:K]
+        tot += int(np.sum(dd <= ex_d[r, K - 1]))
+    return tot / (G.n * K)
+
+
+CASES = [("uniform", 12000, 16, "euclidean", dict(K=25, L=50, S=10)),
+         ("mixture", 12000, 32, "euclidean", dict(K=20, L=40, S=10)),
+         ("sphere", 10000, 24, "angular", dict(K=15, L=40, S=8)),
+         ("uniform", 8000, 20, "l2sqr", dict(K=10, L=30, S=8))]
+
+
+@pytest.mark.parametrize("kind,n,d,metric,bp", CASES)
+def test_build_recall_matches_reference(gpu_ctx, kind, n, d, metric, bp):
+    X = data(kind, n, d, n + d)
+    gpu_ctx.set_data(X, metric)
+    info = gpu_ctx.build(iterations=30, reverse=0, **bp)
+    off, ids, dists, M = gpu_ctx.graph()
+    G = ko.Graph(off, ids, dists, M)
+    K = bp["K"]
+    # exact K-NN (self excluded) and the two graphs' recall
+    c2 = __import__("kgraph_b200.capi", fromlist=["capi"]).Context(0)
+    c2.set_data(X, metric)
+    ex_i, ex_d = exact_knn(c2, X, K)
+    c2.close()
+    R, rinfo, rlog = ko.Oracle(X, metric).build(iterations=30, reverse=0, **bp)
+    r_gpu = graph_recall(G, ex_d, K)
+    r_ref = graph_recall(R, ex_d, K)
+    assert abs(r_gpu - r_ref) <= 0.005, (r_gpu, r_ref, info, rinfo)
+    # deterministic invariants: sorted rows, no duplicate ids, canonical distances, M <= L
+    o = ko.Oracle(X, metric)
+    rng = np.random.default_rng(0)
+    for r in rng.choice(n, 200, replace=False):
+        a, b = int(off[r]), int(off[r + 1])
+        row_i, row_d = ids[a:b], dists[a:b]
+        assert (np.diff(row_d) >= 0).all()
+        assert len(set(row_i.tolist())) == len(row_i)
+        for j in range(0, len(row_i), 7):
+            assert bits(np.float32(o.pair(r, row_i[j]))) == bits(row_d[j])
+    assert (M <= bp["L"]).all() and (M >= 1).all()
+
+
+def test_build_info_and_errors(gpu_ctx):
+    from kgraph_b200 import capi
+    X = data("uniform", 3000, 16, 1)
+    gpu_ctx.set_data(X, "euclidean")
+    info = gpu_ctx.build(K=10, L=30, S=8, iterations=2)
+    assert info["iterations"] == 2 and info["stop_condition"] == 0
+    info = gpu_ctx.build(K=10, L=30, S=8, iterations=30, recall=0.9)
+    assert info["stop_condition"] in (1, 2) and info["recall"] > 0.5
+    small = capi.Context(0)
+    small.set_data(X[:10], "euclidean")
+    with pytest.raises(capi.KGError, match="K larger than dataset size"):
+        small.build(K=10)
+    with pytest.raises(capi.KGError, match="prune level not supported"):
+        gpu_ctx.build(K=10, L=30, S=8, prune=3)
+    small.close()
+
+
+@pytest.mark.parametrize("name,rev", [("ang20", -1), ("ang20", 5), ("ang20", 100), ("mix32", -1)])
+def test_reverse_matches_reference_exactly(gpu_ctx, name, rev):
+    g = load_golden(name)
+    G = ko.read_index(g["index_bytes"])
+    gpu_ctx.set_data(g["X"], g["metric"])
+    gpu_ctx.set_graph(G.offsets, G.ids, G.dists, G.M)
+    gpu_ctx.reverse(rev)
+    off, ids, dists, M = gpu_ctx.graph()
+    R = ko.Oracle(g["X"], g["metric"]).reverse(G, rev)
+    assert (off == R.offsets).all()
+    assert (ids == R.ids).all()
+    assert (bits(dists) == bits(R.dists)).all()
+    assert (M == R.M).all()
+
+
+@pytest.mark.parametrize("level", [1, 2, 3])
+def test_prune_matches_reference_exactly(gpu_ctx, level):
+    g = load_golden("ang20")
+    G = ko.read_index(g["index_bytes"])
+    gpu_ctx.set_data(g["X"], g["metric"])
+    gpu_ctx.set_graph(G.offsets, G.ids, G.dists, G.M)
+    gpu_ctx.prune(level)
+    off, ids, dists, M = gpu_ctx.graph()
+    R = ko.Oracle(g["X"], g["metric"]).prune(G, level)
+    assert (off == R.offsets).all() and (ids == R.ids).all() and (M == R.M).all()
+
+
+def test_build_then_search_python_module(tmp_path):
+    import kgraph_b200 as kgraph
+    X = data("uniform", 20000, 16, 3)
+    Q = data("uniform", 500, 16, 4)
+    k = kgraph.KGraph(X, "euclidean")
+    k.build(K=25, L=50, S=10, reverse=-1)
+    ids, d = k.search(Q, K=10, P=100, withDistance=True)
+    bf, bd = kgraph.KGraph(X, "euclidean").search(Q, K=10, withDistance=True)
+    hit = np.mean([np.sum(d[q] <= bd[q, -1]) / 10 for q in range(len(Q))])
+    assert hit > 0.98
+    p = tmp_path / "g.idx"
+    k.save(str(p))
+    k2 = kgraph.KGraph(X, "euclidean")
+    k2.load(str(p))
+    i2, d2 = k2.search(Q, K=10, P=100, withDistance=True)
+    assert (i2 == ids).all() and (bits(d2) == bits(d)).all()
