@@ -142,7 +142,9 @@ __global__ void __launch_bounds__(256) init_kernel(BuildState s) {
 // reference's value: pool.size() when the radius test rejects, L+1 for a
 // duplicate, else the insert position.
 __device__ uint32_t locked_insert(const BuildState &s, uint32_t x, uint32_t y, float d, int lane) {
-    float rad = *reinterpret_cast<volatile float *>(s.radius + x);
+    float rad = 0.f;
+    if (lane == 0) rad = *reinterpret_cast<volatile float *>(s.radius + x);
+    rad = __shfl_sync(FULL, rad, 0);   // one read, the same decision in every lane
     if (d > rad) return s.Lp;
     uint32_t ok = 1;
     if (lane == 0) {
@@ -157,7 +159,9 @@ __device__ uint32_t locked_insert(const BuildState &s, uint32_t x, uint32_t y, f
     __threadfence();
     volatile float *pd = s.pool_d + (size_t)x * s.PS;
     volatile uint32_t *pi = s.pool_i + (size_t)x * s.PS;
-    const uint32_t Lc = *reinterpret_cast<volatile uint32_t *>(s.nodeL + x);
+    uint32_t Lc = 0;
+    if (lane == 0) Lc = *reinterpret_cast<volatile uint32_t *>(s.nodeL + x);
+    Lc = __shfl_sync(FULL, Lc, 0);
     uint32_t r = warp_update_knn(pd, pi, (uint32_t *)nullptr, Lc, d, y | FLAG_BIT, 0u, lane);
     if (r <= Lc) {
         if (Lc + 1 < s.Lp) {

@@ -43,6 +43,7 @@ int check_device_error(kg_ctx *ctx, const char *what) {
     if (w & ERR_LOCK_TIMEOUT) m += " lock-spin limit reached;";
     if (w & ERR_CAPACITY) m += " list capacity exceeded;";
     if (w & ERR_BAD_ID) m += " node id out of range;";
+    if (w & ERR_STEP_LIMIT) m += " search step bound exceeded;";
     if (w & ERR_INIT_K) { return set_error(ctx, KG_E_INVALID, "L < params.K"); }
     return set_error(ctx, KG_E_DEVICE, m);
 }

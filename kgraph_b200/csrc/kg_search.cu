@@ -223,9 +223,17 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a) {
             __syncwarp();
 
             uint32_t k = 0;
+            // Each expansion advances m or clears a flag of an entry that was inserted
+            // once, so the walk ends; the bound only turns a defect into an error.
+            const uint64_t step_limit = 64ull * (N + cap) + 4096;
+            uint64_t steps = 0;
             while (true) {
                 k = warp_next_flagged(s.pid, k, L, lane);
                 if (k >= L) break;
+                if (++steps > step_limit) {
+                    if (lane == 0) raise_error(a.err, ERR_STEP_LIMIT);
+                    break;
+                }
                 const uint32_t idf = s.pid[k];
                 const uint32_t mM = s.pm[k];
                 const uint32_t beginM = mM & 0xFFFFu, eM = mM >> 16;
@@ -246,8 +254,9 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a) {
                     if (__any_sync(FULL, bad)) { if (lane == 0) raise_error(a.err, ERR_BAD_ID); }
                     act = act && !bad;
                     // first occurrence within this chunk, in adjacency order
-                    unsigned same = __match_any_sync(FULL, id);
-                    bool first = act && ((__ffs(same & __ballot_sync(FULL, act)) - 1) == lane);
+                    const unsigned same = __match_any_sync(FULL, id);
+                    const unsigned actm = __ballot_sync(FULL, act);   // every lane votes: no short-circuit
+                    const bool first = act && ((__ffs(same & actm) - 1) == lane);
                     bool isnew = false;
                     if (first) isnew = !visited_test_set(vis, id);
                     unsigned nm = __ballot_sync(FULL, isnew);
