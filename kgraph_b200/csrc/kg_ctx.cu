@@ -265,15 +265,13 @@ int kg_search_batch(kg_ctx *ctx, const float *queries, size_t nq, size_t q_strid
         hP.resize(Q);
         cudaMemcpy(hP.data(), P_per_q, Q * sizeof(uint32_t), cudaMemcpyDefault);
     }
-    uint32_t Kmax = params->K, Pmax = params->P;
+    uint32_t Kmax = params->K;
     if (K_per_q) Kmax = *std::max_element(hK.begin(), hK.end());
-    if (P_per_q) Pmax = *std::max_element(hP.begin(), hP.end());
     if (Kmax > out_ld) return set_error(ctx, KG_E_INVALID, "out_ld smaller than K");
     if (params->init && params->init > out_ld) return set_error(ctx, KG_E_INVALID, "init larger than out_ld");
 
     // without an index every query is a brute-force query (python-api.cpp:303-314)
     const uint32_t Pforce = graph ? 0u : N;
-    uint32_t effPmax = graph ? Pmax : N;
     // seed table: for each distinct P < N, T lists of P ids from mt19937(seed)
     unsigned seed = params->seed;
     if (seed == 0) seed = (unsigned)time(NULL);
@@ -313,7 +311,19 @@ int kg_search_batch(kg_ctx *ctx, const float *queries, size_t nq, size_t q_strid
     a.init = graph ? params->init : 0u;
     a.epsilon = params->epsilon;
     a.out_ld = (uint32_t)out_ld;
-    a.cap = Kmax + effPmax + 1;
+    // pool capacity: K+P+1 for a walk (kgraph.cpp:434), K+1 for a brute-force query (P >= N)
+    uint32_t cap = Kmax + 1;
+    if (graph) {
+        if (P_per_q || K_per_q) {
+            for (size_t i = 0; i < Q; ++i) {
+                uint32_t P = P_per_q ? hP[i] : params->P, K = K_per_q ? hK[i] : params->K;
+                if (P < N) cap = std::max(cap, K + P + 1);
+            }
+        } else if (params->P < N) {
+            cap = params->K + params->P + 1;
+        }
+    }
+    a.cap = cap;
     a.rcap = Kmax + 1;
     if (search_warp_smem_bytes(ld, a.cap, a.rcap) > 200 * 1024)
         return set_error(ctx, KG_E_INVALID, "K + P too large for one query's shared-memory pool");
