@@ -110,6 +110,27 @@ int kg_reverse(kg_ctx *ctx, int rev_k);
 /* KGraph::prune (kgraph.h:180; kgraph.cpp:584-665) on the current graph. */
 int kg_prune(kg_ctx *ctx, unsigned level);
 
+/* kg_search_batch without any device allocation.  No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc while serving
+ * -- a latency-critical thread that must not block on the allocator, or an
+ * application that owns all GPU memory through its own pool.  Queries and
+ * outputs must be DEVICE buffers (queries: 16-byte aligned rows of the
+ * context's padded width, q_stride_bytes = 4 * round_up(d, 16)); dataset and
+ * graph are the context's.  One K and P for the whole batch, P <= 4096.
+ * Scratch (counters, seed table, visited sets) is a static device array of
+ * KG_NOALLOC_SCRATCH_BYTES per GPU, held until the process exits; a batch
+ * whose seeds, per-query index and one SM's worth of visited sets do not fit
+ * is rejected with KG_E_INVALID.  The first call on a device looks up the
+ * array's device address, so make it before any stream capture.  Every call
+ * shares the array: calls whose kernels overlap on the GPU race; serialise
+ * them.  Results are those of kg_search_batch. */
+#define KG_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)
+int kg_search_batch_noalloc(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes,
+                            const kg_search_params *params, size_t out_ld, uint32_t *ids, float *dists,
+                            uint32_t *counts, float *costs);
+/* Size of that static scratch array in bytes. */
+size_t kg_noalloc_scratch_bytes(void);
+
 /* Milliseconds of the last kg_build / kg_search_batch device work, measured
  * with CUDA events on the context's stream (for profiling and benchmarks). */
 int kg_last_timing(kg_ctx *ctx, float *build_ms, float *search_ms);

@@ -19,7 +19,7 @@ SYMBOLS = [
     "kg_index_params_default", "kg_search_params_default", "kg_ctx_create", "kg_ctx_destroy",
     "kg_last_error", "kg_version", "kg_set_verbosity", "kg_set_data", "kg_build", "kg_graph_size",
     "kg_graph_export", "kg_graph_import", "kg_search_batch", "kg_reverse", "kg_prune", "kg_last_timing",
-    "kg_last_search_work",
+    "kg_last_search_work", "kg_search_batch_noalloc", "kg_noalloc_scratch_bytes",
 ]
 
 
@@ -66,6 +66,8 @@ def lib():
         L.kg_prune.argtypes = [vp, C.c_uint]
         L.kg_last_timing.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_float)]
         L.kg_last_search_work.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+        L.kg_search_batch_noalloc.argtypes = [vp, vp, sz, sz, C.POINTER(SearchParams), sz, vp, vp, vp, vp]
+        L.kg_noalloc_scratch_bytes.restype = sz
         L.kg_index_params_default.argtypes = [C.POINTER(IndexParams)]
         L.kg_search_params_default.argtypes = [C.POINTER(SearchParams)]
         _lib = L
@@ -175,6 +177,11 @@ class Context:
         """kg_search_batch on raw (device or host) pointers."""
         self._check(self.L.kg_search_batch(self.h, q_ptr, nq, q_stride, C.byref(params), kq_ptr, pq_ptr, out_ld,
                                            ids_ptr, d_ptr, c_ptr, cost_ptr))
+
+    def search_noalloc(self, q_ptr, nq, q_stride, params, out_ld, ids_ptr, d_ptr, c_ptr, cost_ptr):
+        """kg_search_batch_noalloc on device pointers (no device allocation)."""
+        self._check(self.L.kg_search_batch_noalloc(self.h, q_ptr, nq, q_stride, C.byref(params), out_ld, ids_ptr,
+                                                   d_ptr, c_ptr, cost_ptr))
 
     def reverse(self, k):
         self._check(self.L.kg_reverse(self.h, k))
