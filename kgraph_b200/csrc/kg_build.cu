@@ -705,6 +705,7 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
     ctx->E = E;
     ctx->no_dist = false;
     ctx->has_graph = true;
+    ++ctx->graph_version;
     int de = check_device_error(ctx, "build");
     if (de != KG_OK) return de;
     if (params->reverse) {

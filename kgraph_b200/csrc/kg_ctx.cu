@@ -82,6 +82,28 @@ __global__ void norms_kernel(DataView D, float *norms) {
     }
 }
 
+__global__ void maxdeg_kernel(uint32_t N, const uint64_t *off, uint32_t *out) {
+    uint32_t m = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+        m = max(m, (uint32_t)(off[i + 1] - off[i]));
+    for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+// ELL copy of the first W neighbours of every node and its {M, degree}.
+__global__ void ell_kernel(uint32_t N, const uint64_t *off, const uint32_t *nbr, const uint32_t *M, uint32_t W,
+                           uint32_t *ell, uint2 *meta) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t n = w; n < N; n += nw) {
+        const uint64_t o = off[n];
+        const uint32_t deg = (uint32_t)(off[n + 1] - o);
+        const uint32_t c = min(deg, W);
+        for (uint32_t p = lane; p < c; p += 32) ell[(size_t)n * W + p] = nbr[o + p];
+        if (lane == 0) meta[n] = make_uint2(M[n], deg);
+    }
+}
+
 struct Lock {
     kg_ctx *c;
     explicit Lock(kg_ctx *ctx) : c(ctx) { c->mu.lock(); cudaSetDevice(c->device); }
@@ -128,7 +150,7 @@ void kg_ctx_destroy(kg_ctx *c) {
     if (!c) return;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
-    DevBuf *bufs[] = {&c->X, &c->norms, &c->offsets, &c->nbr, &c->nbr_d, &c->Mnode, &c->errw, &c->counter,
+    DevBuf *bufs[] = {&c->X, &c->norms, &c->offsets, &c->nbr, &c->nbr_d, &c->Mnode, &c->errw, &c->counter, &c->ell, &c->meta,
                       &c->visited, &c->qbuf, &c->kbuf, &c->pbuf, &c->seeds, &c->seed_index, &c->init_ids,
                       &c->out_ids, &c->out_d, &c->out_cnt, &c->out_cost};
     for (DevBuf *b : bufs) b->release();
@@ -236,8 +258,35 @@ int kg_graph_import(kg_ctx *ctx, size_t n, const uint64_t *offsets, const uint32
     ctx->E = E;
     ctx->no_dist = dists == nullptr;
     ctx->has_graph = true;
+    ++ctx->graph_version;
     return KG_OK;
 }
+
+namespace kgb {
+// Builds the search-side graph layout when the graph changed since the last search.
+int ensure_search_layout(kg_ctx *ctx) {
+    if (!ctx->has_graph || ctx->layout_version == ctx->graph_version) return KG_OK;
+    const uint32_t N = ctx->gn;
+    cudaError_t e;
+    uint32_t *dmax = ctx->counter.as<uint32_t>() + 12;
+    cudaMemsetAsync(dmax, 0, 4, ctx->stream);
+    maxdeg_kernel<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(N, ctx->offsets.as<uint64_t>(), dmax);
+    uint32_t maxdeg = 0;
+    cudaMemcpyAsync(&maxdeg, dmax, 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "layout");
+    uint32_t W = std::min<uint32_t>(128, std::max<uint32_t>(32, (maxdeg + 31) / 32 * 32));
+    if ((e = ctx->ell.reserve((size_t)N * W * 4 + 4)) != cudaSuccess ||
+        (e = ctx->meta.reserve((size_t)N * 8 + 8)) != cudaSuccess)
+        return cuda_fail(ctx, e, "alloc search layout");
+    ell_kernel<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(N, ctx->offsets.as<uint64_t>(), ctx->nbr.as<uint32_t>(),
+                                                           ctx->Mnode.as<uint32_t>(), W, ctx->ell.as<uint32_t>(),
+                                                           ctx->meta.as<uint2>());
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "layout");
+    ctx->ell_w = W;
+    ctx->layout_version = ctx->graph_version;
+    return KG_OK;
+}
+}  // namespace kgb
 
 int kg_search_batch(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes,
                     const kg_search_params *params, const uint32_t *K_per_q, const uint32_t *P_per_q,
@@ -305,6 +354,13 @@ int kg_search_batch(kg_ctx *ctx, const float *queries, size_t nq, size_t q_strid
     a.offsets = graph ? ctx->offsets.as<uint64_t>() : nullptr;
     a.nbr = graph ? ctx->nbr.as<uint32_t>() : nullptr;
     a.Mnode = graph ? ctx->Mnode.as<uint32_t>() : nullptr;
+    if (graph) {
+        int lr = ensure_search_layout(ctx);
+        if (lr != KG_OK) return lr;
+        a.ell = ctx->ell.as<uint32_t>();
+        a.ell_w = ctx->ell_w;
+        a.meta = ctx->meta.as<uint2>();
+    }
     a.nq = (uint32_t)Q;
     a.q_ld = ld;
     a.K = params->K; a.P = graph ? params->P : Pforce; a.Mp = params->M; a.S = params->S; a.T = params->T;

@@ -57,6 +57,12 @@ struct kg_ctx {
     uint32_t gn = 0;
     bool has_graph = false;
     bool no_dist = false;
+    uint64_t graph_version = 0;      // bumped whenever the graph changes
+
+    // search-side copy of the graph: ELL rows of the first ell_w neighbours + {M, degree}
+    kgb::DevBuf ell, meta;
+    uint32_t ell_w = 0;
+    uint64_t layout_version = ~0ull;
 
     // scratch
     kgb::DevBuf errw, counter, visited, qbuf, kbuf, pbuf, seeds, seed_index, init_ids, out_ids, out_d,

@@ -237,6 +237,7 @@ int graph_reverse(kg_ctx *ctx, int rev_k) {
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return fail("reverse");
     swap_graph(ctx, foff, fi, fd);
     ctx->E = Efin;
+    ++ctx->graph_version;
     DevBuf *all[] = {&kcnt, &koff, &rc, &toff, &deg, &noff, &fdeg, &foff, &key, &val, &skey, &sval, &tmp,
                      &ai, &ad, &fi, &fd};
     for (DevBuf *b : all) b->release();
@@ -267,6 +268,7 @@ static int prune1(kg_ctx *ctx) {
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "prune");
     swap_graph(ctx, noff, ni, nd);
     ctx->E = E;
+    ++ctx->graph_version;
     return KG_OK;
 }
 
@@ -319,6 +321,7 @@ static int prune2(kg_ctx *ctx) {
     cudaMemcpy(ctx->nbr.p, ids.data(), ctx->E * 4, cudaMemcpyHostToDevice);
     if (!ctx->no_dist) cudaMemcpy(ctx->nbr_d.p, ds.data(), ctx->E * 4, cudaMemcpyHostToDevice);
     cudaMemcpy(ctx->Mnode.p, newL.data(), N * 4, cudaMemcpyHostToDevice);
+    ++ctx->graph_version;
     return prune1(ctx);
 }
 

@@ -69,8 +69,22 @@ __device__ __forceinline__ WarpSmem carve(char *base, const SearchArgs &a) {
 
 // actual_M (kgraph.cpp:284-286) as stored in NeighborX::M (uint16_t).
 __device__ __forceinline__ uint32_t actual_M(const SearchArgs &a, uint32_t pM, uint32_t id) {
-    uint32_t deg = (uint32_t)(a.offsets[id + 1] - a.offsets[id]);
-    return min(max(a.Mnode[id], pM), deg) & 0xFFFFu;
+    uint32_t deg, M;
+    if (a.meta) {
+        uint2 md = a.meta[id];
+        M = md.x;
+        deg = md.y;
+    } else {
+        deg = (uint32_t)(a.offsets[id + 1] - a.offsets[id]);
+        M = a.Mnode[id];
+    }
+    return min(max(M, pM), deg) & 0xFFFFu;
+}
+
+// Neighbour p of node: the ELL copy for p < ell_w, else the CSR.
+__device__ __forceinline__ uint32_t neighbour(const SearchArgs &a, uint32_t node, uint32_t p) {
+    if (a.ell && p < a.ell_w) return a.ell[(size_t)node * a.ell_w + p];
+    return a.nbr[a.offsets[node] + p];
 }
 
 // Distances for cnt candidates cid[0..cnt) -> cd[], 8 per pass (4-lane groups).
@@ -106,6 +120,27 @@ __device__ uint32_t warp_bruteforce(const SearchArgs &a, const WarpSmem &s, floa
         __syncwarp();
     }
     return L;
+}
+
+// Distances of the candidate lanes in `cm` (each holds its id), computed 8 at a
+// time by the 4-lane groups; every candidate lane returns its own distance.
+// Everything stays in registers (no shared-memory staging, so no barrier waits
+// on memory operations still in flight).
+__device__ __forceinline__ float warp_cand_dist(const SearchArgs &a, const float *q, float qn, unsigned cm, bool cand,
+                                               uint32_t id, int lane) {
+    const int g = lane >> 2, t = lane & 3;
+    const uint32_t n = __popc(cm);
+    const uint32_t my = __popc(cm & ((1u << lane) - 1u));
+    float mine = 0.f;
+    for (uint32_t base = 0; base < n; base += 8) {
+        const uint32_t i = base + g;
+        const int src = i < n ? (int)__fns(cm, 0, i + 1) : 0;
+        const uint32_t cid = __shfl_sync(FULL, id, src);
+        const float dd = query_dist(a.D, q, qn, i < n ? cid : 0u, t, FULL);
+        const float got = __shfl_sync(FULL, dd, (int)(4 * (my & 7)));
+        if (cand && (my >> 3) == (base >> 3)) mine = got;
+    }
+    return mine;
 }
 
 __device__ __forceinline__ bool visited_test_set(uint32_t *vis, uint32_t id) {
@@ -227,58 +262,105 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a) {
             // once, so the walk ends; the bound only turns a defect into an error.
             const uint64_t step_limit = 64ull * (N + cap) + 4096;
             uint64_t steps = 0;
+            // The expansion loop of kgraph.cpp:478-514.  The entry at k is expanded
+            // batch after batch (S neighbours each) exactly as the reference's loop
+            // does while no insert lands at or before k.  Its adjacency entries come
+            // in windows of up to 128 (four per lane) with one round trip for the
+            // ids and one for their visited bits (this warp's private set, so the
+            // bits can only change by this walk); a batch's unvisited neighbours are
+            // then confirmed with an atomic test-and-set (exact even when an id
+            // recurs across chunks), their distances computed and inserted in one
+            // merge.  When an insert lands at or before k the reference moves on to
+            // another entry: so does this loop, and the window is dropped (it is
+            // reloaded from m when the entry comes up again).
             while (true) {
                 k = warp_next_flagged(s.pid, k, L, lane);
                 if (k >= L) break;
-                if (++steps > step_limit) {
-                    if (lane == 0) raise_error(a.err, ERR_STEP_LIMIT);
-                    break;
-                }
-                const uint32_t idf = s.pid[k];
-                const uint32_t mM = s.pm[k];
-                const uint32_t beginM = mM & 0xFFFFu, eM = mM >> 16;
-                uint32_t endM = beginM + S;
-                uint32_t nidf = idf;
-                if (endM > eM) { nidf = idf & ID_MASK; endM = eM; }   // kgraph.cpp:487-490
-                __syncwarp();
-                if (lane == 0) { s.pid[k] = nidf; s.pm[k] = (endM & 0xFFFFu) | (eM << 16); }
-                __syncwarp();
-                const uint32_t node = idf & ID_MASK;
-                const uint64_t nb = a.offsets[node];
-                n_adj += endM - beginM;
-                for (uint32_t m0 = beginM; m0 < endM; m0 += 32) {
-                    const uint32_t cnt = min(32u, endM - m0);
-                    bool act = lane < (int)cnt;
-                    uint32_t id = act ? a.nbr[nb + m0 + lane] : 0xFFFFFFFFu;
-                    bool bad = act && id >= N;
-                    if (__any_sync(FULL, bad)) { if (lane == 0) raise_error(a.err, ERR_BAD_ID); }
-                    act = act && !bad;
-                    // first occurrence within this chunk, in adjacency order
-                    const unsigned same = __match_any_sync(FULL, id);
-                    const unsigned actm = __ballot_sync(FULL, act);   // every lane votes: no short-circuit
-                    const bool first = act && ((__ffs(same & actm) - 1) == lane);
-                    bool isnew = false;
-                    if (first) isnew = !visited_test_set(vis, id);
-                    unsigned nm = __ballot_sync(FULL, isnew);
-                    uint32_t nnew = __popc(nm);
-                    if (nnew == 0) continue;
-                    n_comps += nnew;
-                    uint32_t pos = __popc(nm & ((1u << lane) - 1u));
-                    if (isnew) { s.cid[pos] = id; s.cM[pos] = actual_M(a, a.Mp, id); }
-                    __syncwarp();
-                    batch_dist(a, s, qn, nnew, lane);
-                    for (uint32_t c = 0; c < nnew; ++c) {
-                        const float dd = s.cd[c];
-                        const uint32_t cidv = s.cid[c];
-                        uint32_t r = warp_update_knn(s.pd, s.pid, s.pm, L, dd, cidv | FLAG_BIT, 0u, lane);
-                        if (L + 1 < cap) ++L;
-                        if (r < L) {
-                            if (lane == 0) s.pm[r] = (s.pm[r] & 0xFFFFu) | (s.cM[c] << 16);
-                            if (r < k) k = r;
-                        }
-                        __syncwarp();
+                const uint32_t node = s.pid[k] & ID_MASK;
+                const uint32_t mM0 = s.pm[k];
+                const uint32_t eM = mM0 >> 16;
+                uint32_t m = mM0 & 0xFFFFu;
+                uint32_t wlo = 0, whi = 0;   // loaded window [wlo, whi)
+                uint32_t wid[4];
+                bool wuv[4];
+                bool moved = false;
+                while (true) {
+                    if (++steps > step_limit) {
+                        if (lane == 0) raise_error(a.err, ERR_STEP_LIMIT);
+                        k = L;
+                        break;
                     }
+                    // kgraph.cpp:485-491: the entry's next batch
+                    const uint32_t beginM = m;
+                    uint32_t endM = beginM + S;
+                    const bool done = endM > eM;
+                    if (done) endM = eM;
+                    if (lane == 0) {
+                        if (done) s.pid[k] = s.pid[k] & ID_MASK;
+                        s.pm[k] = (endM & 0xFFFFu) | (eM << 16);
+                    }
+                    __syncwarp();
+                    n_adj += endM - beginM;
+                    // kgraph.cpp:495-513, in pieces that stay inside one 32-entry chunk
+                    for (uint32_t p0 = beginM; p0 < endM;) {
+                        if (p0 < wlo || p0 >= whi) {   // load the window that starts at p0
+                            wlo = p0;
+                            whi = min(p0 + 128u, eM);
+#pragma unroll
+                            for (int c = 0; c < 4; ++c) {
+                                const uint32_t p = wlo + 32 * c + lane;
+                                const bool act = p < whi;
+                                uint32_t id = act ? neighbour(a, node, p) : 0xFFFFFFFFu;
+                                const bool bad = act && id >= N;
+                                if (__any_sync(FULL, bad)) { if (lane == 0) raise_error(a.err, ERR_BAD_ID); }
+                                const bool ok = act && !bad;
+                                const unsigned same = __match_any_sync(FULL, id);
+                                const unsigned okm = __ballot_sync(FULL, ok);   // every lane votes
+                                wid[c] = id;
+                                wuv[c] = ok && ((__ffs(same & okm) - 1) == lane);
+                            }
+#pragma unroll
+                            for (int c = 0; c < 4; ++c)   // first occurrences not yet visited
+                                if (wuv[c]) wuv[c] = !((__ldcg(vis + (wid[c] >> 5)) >> (wid[c] & 31)) & 1u);
+                        }
+                        const uint32_t c = (p0 - wlo) >> 5;
+                        const uint32_t cbase = wlo + 32 * c;
+                        const uint32_t p1 = min(endM, cbase + 32);
+                        const uint32_t lo = p0 - cbase, hi = p1 - cbase;
+                        uint32_t id = 0;
+                        bool uv = false;
+#pragma unroll
+                        for (int cc = 0; cc < 4; ++cc)
+                            if ((uint32_t)cc == c) { id = wid[cc]; uv = wuv[cc]; }
+                        const bool cand = uv && (uint32_t)lane >= lo && (uint32_t)lane < hi;
+                        const unsigned cm = __ballot_sync(FULL, cand);
+                        if (cm) {
+                            // All three in flight together: the exact test-and-set of the
+                            // visited bit, the candidate's {M, degree}, and its row (distance).
+                            bool isnew = false;
+                            uint32_t aM = 0;
+                            if (cand) {
+                                const uint32_t bit = 1u << (id & 31);
+                                isnew = !(atomicOr(vis + (id >> 5), bit) & bit);
+                                aM = actual_M(a, a.Mp, id);
+                            }
+                            const float dd = warp_cand_dist(a, s.q, qn, cm, cand, id, lane);
+                            const unsigned nm = __ballot_sync(FULL, isnew);
+                            if (nm) {
+                                n_comps += __popc(nm);
+                                uint32_t mr;   // new entries: flag set, m = 0, M = actual_M
+                                L = warp_batch_insert(s.pd, s.pid, s.pm, L, cap, nm, dd, id | FLAG_BIT, aM << 16,
+                                                      &mr, lane);
+                                if (mr <= k) moved = true;   // the expanded entry is no longer at k
+                                if (mr < k) k = mr;
+                            }
+                        }
+                        p0 = p1;
+                    }
+                    m = endM;
+                    if (done || moved) break;   // the loop head picks the reference's next k
                 }
+                if (k >= L) break;
             }
             if (L > K) L = K;   // kgraph.cpp:515
             if (!have_results) {

@@ -11,6 +11,9 @@ struct SearchArgs {
     const uint64_t *offsets;    // CSR graph: n+1 offsets
     const uint32_t *nbr;        // neighbour ids
     const uint32_t *Mnode;      // per-node M (KGraphImpl::M)
+    const uint32_t *ell;        // optional: the first ell_w neighbours of every node, node-major
+    uint32_t ell_w;
+    const uint2 *meta;          // optional: per node {M, degree} (saves the offsets loads)
     const float *Q;             // queries, nq rows of q_ld (= D.ld) floats
     uint32_t q_ld, nq;
     const uint32_t *Kq, *Pq;    // optional per-query K and P (null: use K, P)

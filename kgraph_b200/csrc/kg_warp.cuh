@@ -69,6 +69,72 @@ __device__ __forceinline__ uint32_t warp_update_knn(PD pd, PI pid, uint32_t *pm,
     return i;
 }
 
+// n successive UpdateKnnList calls (kgraph.cpp:503-512) by one warp in one
+// pass.  The candidates are the lanes set in `mask`, in lane order; each such
+// lane holds its candidate's distance di, id-with-flag idf and m|M word pmv.
+// They are inserted in order into the sorted pool pd/pid/pm of length L whose
+// capacity is cap (slot cap-1 is the overflow slot), L growing by one per
+// candidate up to cap-1.  Their ids are distinct and absent from the pool (the
+// caller's visited set guarantees it), so the duplicate rule never fires.
+// Sequential inserts with insert-after-equals and eviction of the last entry
+// produce exactly the stable merge of the pool with the candidates ordered by
+// (distance, order), truncated to the final length; candidate i's position at
+// the moment it is inserted is a_i + #{j < i : d_j <= d_i}, a_i = #pool
+// entries <= d_i.  Returns the new L; *min_rank receives the smallest insertion
+// position among candidates that entered the list (r < L after the increment),
+// or 0xFFFFFFFF.
+__device__ __forceinline__ uint32_t warp_batch_insert(float *pd, uint32_t *pid, uint32_t *pm, uint32_t L,
+                                                      uint32_t cap, unsigned mask, float di, uint32_t idf,
+                                                      uint32_t pmv, uint32_t *min_rank, int lane) {
+    const uint32_t n = __popc(mask);
+    const bool me = (mask >> lane) & 1u;
+    const uint32_t my = __popc(mask & ((1u << lane) - 1u));   // this lane's candidate index
+    uint32_t ai = 0;
+    if (me) {   // upper bound of di in pd[0, L)
+        uint32_t lo = 0, hi = L;
+        while (lo < hi) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (pd[mid] <= di) lo = mid + 1; else hi = mid;
+        }
+        ai = lo;
+    }
+    uint32_t e = 0, f = 0, mina = me ? ai : 0xFFFFFFFFu;
+    for (unsigned rest = mask; rest; rest &= rest - 1) {
+        const int src = __ffs(rest) - 1;
+        const float dj = __shfl_sync(FULL, di, src);
+        const uint32_t j = __popc(mask & ((1u << src) - 1u));
+        if (j < my && dj <= di) ++e;
+        if (dj < di || (dj == di && j < my)) ++f;
+    }
+    const uint32_t r = ai + e;   // position when this candidate is inserted
+    const bool ins = me && r < min(L + my + 1, cap - 1);
+    uint32_t mr = ins ? r : 0xFFFFFFFFu;
+    for (int o = 16; o; o >>= 1) {
+        mr = min(mr, __shfl_xor_sync(FULL, mr, o));
+        mina = min(mina, __shfl_xor_sync(FULL, mina, o));
+    }
+    *min_rank = mr;
+    const uint32_t Lf = min(L + n, cap - 1);
+    // move pool entries q >= mina up by #{j : a_j <= q}, top-down (each chunk's
+    // loads precede the next chunk's stores, which reach at most this chunk)
+    for (int top = (int)L - 1; top >= (int)mina; top -= 32) {
+        const int q = top - lane;
+        const bool act = q >= (int)mina;
+        float dv = 0.f;
+        uint32_t iv = 0, mv = 0, sh = 0;
+        if (act) { dv = pd[q]; iv = pid[q]; mv = pm[q]; }
+        for (unsigned rest = mask; rest; rest &= rest - 1)
+            sh += (__shfl_sync(FULL, ai, __ffs(rest) - 1) <= (uint32_t)q) ? 1u : 0u;
+        __syncwarp();
+        if (act && (uint32_t)q + sh < Lf) { pd[q + sh] = dv; pid[q + sh] = iv; pm[q + sh] = mv; }
+    }
+    __syncwarp();
+    const uint32_t fpos = ai + f;
+    if (me && fpos < Lf) { pd[fpos] = di; pid[fpos] = idf; pm[fpos] = pmv; }
+    __syncwarp();
+    return Lf;
+}
+
 // First index >= k in [0, L) whose flag bit is set; L if none.
 __device__ __forceinline__ uint32_t warp_next_flagged(const uint32_t *pid, uint32_t k, uint32_t L, int lane) {
     for (uint32_t base = k; base < L; base += 32) {
