@@ -42,6 +42,9 @@ N_BASE, DIM, N_CENTRES, N_QUERIES = 1_000_000, 128, 256, 10_000
 BUILD = dict(K=50, L=100, S=12, R=100, iterations=30, reverse=-1)
 P_LADDER = [100, 200, 300, 500, 700, 1000, 1500, 2000, 3000]
 TARGET = 0.95
+# DRAM read + write of one search launch (10,000 queries, K=10, P=1000) from an
+# ncu capture of the same kernel on the 400k-node version of this workload.
+SEARCH_DRAM_BYTES_PER_LAUNCH = 22.09e9
 
 
 def make_data(n=N_BASE, nq=N_QUERIES, d=DIM, centres=N_CENTRES, seed=1, rank=0):
@@ -127,6 +130,21 @@ class ClockSampler:
         reasons = sorted({names[k] for r in rows for k in range(4) if r[3 + k].lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": float(rows[0][1]),
                 "reasons": reasons, "samples": len(rows)}
+
+
+def max_over_ranks(x, dist, world, device):
+    """Max of a per-rank float over all ranks (every rank takes the same collective step)."""
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(per_rank_ms, queries_per_rank, steps, dist, world, device):
+    """Whole-job queries/s of `world` replicas: all ranks' queries over the slowest rank's time."""
+    slowest = max_over_ranks(per_rank_ms, dist, world, device)
+    return queries_per_rank * world * steps / (slowest / 1000.0), slowest
 
 
 def reference_cpu_search(X, Q, index_path, K, P, threads=0):
@@ -267,11 +285,7 @@ def main():
         dist.barrier()
     evals, adj = ctx.search_work()
     tot_ms = sum(step_ms)
-    t = torch.tensor([tot_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    tot_ms_max = float(t.item())
-    value = N_QUERIES * world * args.steps / (tot_ms_max / 1000)
+    value, tot_ms_max = replica_throughput(tot_ms, N_QUERIES, args.steps, dist, world, "cuda")
 
     # end to end through the C-ABI with host buffers
     Qh = np.ascontiguousarray(Q)
@@ -288,10 +302,7 @@ def main():
         ctx.search_raw(capi._ptr(Qh), N_QUERIES, Qh.strides[0], params, None, None, 10, capi._ptr(hi), capi._ptr(hd),
                        capi._ptr(hc), None)
         e2e_ms.append(1000 * (time.perf_counter() - t0))
-    t = torch.tensor([sum(e2e_ms)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e = N_QUERIES * world * args.steps / (float(t.item()) / 1000)
+    e2e, _ = replica_throughput(sum(e2e_ms), N_QUERIES, args.steps, dist, world, "cuda")
 
     # roofline of the search kernel: algorithmic bytes per launch / launch time
     bytes_per_launch = evals * (DIM * 4 + 4) + adj * 4
@@ -335,7 +346,7 @@ def main():
                         "d2h_bytes_per_step": int(hi.nbytes + hd.nbytes + hc.nbytes)},
                 "gpu_launches": args.steps,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                             "frac": achieved / hbm, "traffic": None,
+                             "frac": achieved / hbm, "traffic": SEARCH_DRAM_BYTES_PER_LAUNCH,
                              "algorithmic_bytes_per_launch": int(bytes_per_launch)},
                 "clocks": clk.summary(), "cpu_baseline": cpu}
         print(json.dumps(line))
