@@ -131,6 +131,43 @@ int kg_search_batch_noalloc(kg_ctx *ctx, const float *queries, size_t nq, size_t
 /* Size of that static scratch array in bytes. */
 size_t kg_noalloc_scratch_bytes(void);
 
+/* Learned entry router.  No counterpart in the reference: it predicts, per
+ * query, starting points for the walk, which the search takes through the
+ * reference's own user-provided starting points (params->init > 0 with the
+ * seeds in ids, doc/params.md "User-Provided Starting Points").  Training
+ * (on the GPU): k-means of the dataset into `clusters` entry clusters (entry
+ * node = the member nearest the centroid); labels = the cluster of the best
+ * node the plain search (P = label_P) finds for each training query; MLP
+ * d -> hidden -> hidden -> clusters (ReLU), BF16 weights with FP32 masters and
+ * accumulation, softmax cross-entropy, Adam. */
+typedef struct {
+    unsigned clusters, hidden, kmeans_iters, label_P, epochs, batch;
+    float lr;
+    unsigned seed;
+} kg_router_params;
+typedef struct {
+    unsigned steps;
+    float final_loss, train_accuracy;
+    unsigned empty_clusters;
+} kg_router_info;
+void kg_router_params_default(kg_router_params *p);
+/* Trains the router on the context's dataset and graph. */
+int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const float *train_queries, size_t ntrain,
+                    size_t q_stride_bytes, kg_router_info *info);
+/* Entry nodes of the m most likely clusters of each query (best first), rows of
+ * out_ld; pass them to kg_search_batch as ids with params->init = m (m < K). */
+int kg_router_seeds(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes, unsigned m, uint32_t *seeds,
+                    size_t out_ld);
+/* Mean loss and gradients (W1|b1|W2|b2|W3|b3, FP32, row-major in x out) of the
+ * MLP on n <= 4096 labelled rows, with `weights` (same layout, may be NULL to
+ * keep the current ones) and identity input normalisation: the check of the
+ * training kernels against an independent implementation. */
+int kg_router_gradients(kg_ctx *ctx, unsigned d, unsigned hidden, unsigned clusters, const float *weights,
+                        const float *x, const int32_t *labels, unsigned n, float *loss, float *grads);
+/* Milliseconds of the last kg_router_seeds device work (CUDA events on the
+ * context's stream). */
+int kg_last_router_timing(kg_ctx *ctx, float *seeds_ms);
+
 /* Milliseconds of the last kg_build / kg_search_batch device work, measured
  * with CUDA events on the context's stream (for profiling and benchmarks). */
 int kg_last_timing(kg_ctx *ctx, float *build_ms, float *search_ms);

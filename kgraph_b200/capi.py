@@ -20,6 +20,7 @@ SYMBOLS = [
     "kg_last_error", "kg_version", "kg_set_verbosity", "kg_set_data", "kg_build", "kg_graph_size",
     "kg_graph_export", "kg_graph_import", "kg_search_batch", "kg_reverse", "kg_prune", "kg_last_timing",
     "kg_last_search_work", "kg_search_batch_noalloc", "kg_noalloc_scratch_bytes",
+    "kg_router_params_default", "kg_router_train", "kg_router_seeds", "kg_router_gradients", "kg_last_router_timing",
 ]
 
 
@@ -32,6 +33,16 @@ class IndexParams(C.Structure):
 class IndexInfo(C.Structure):
     _fields_ = [("stop_condition", C.c_int), ("iterations", C.c_uint), ("cost", C.c_float), ("recall", C.c_float),
                 ("accuracy", C.c_float), ("delta", C.c_float), ("M", C.c_float)]
+
+
+class RouterParams(C.Structure):
+    _fields_ = [("clusters", C.c_uint), ("hidden", C.c_uint), ("kmeans_iters", C.c_uint), ("label_P", C.c_uint),
+                ("epochs", C.c_uint), ("batch", C.c_uint), ("lr", C.c_float), ("seed", C.c_uint)]
+
+
+class RouterInfo(C.Structure):
+    _fields_ = [("steps", C.c_uint), ("final_loss", C.c_float), ("train_accuracy", C.c_float),
+                ("empty_clusters", C.c_uint)]
 
 
 class SearchParams(C.Structure):
@@ -68,6 +79,12 @@ def lib():
         L.kg_last_search_work.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
         L.kg_search_batch_noalloc.argtypes = [vp, vp, sz, sz, C.POINTER(SearchParams), sz, vp, vp, vp, vp]
         L.kg_noalloc_scratch_bytes.restype = sz
+        L.kg_router_params_default.argtypes = [C.POINTER(RouterParams)]
+        L.kg_last_router_timing.argtypes = [vp, C.POINTER(C.c_float)]
+        L.kg_router_train.argtypes = [vp, C.POINTER(RouterParams), vp, sz, sz, C.POINTER(RouterInfo)]
+        L.kg_router_seeds.argtypes = [vp, vp, sz, sz, C.c_uint, vp, sz]
+        L.kg_router_gradients.argtypes = [vp, C.c_uint, C.c_uint, C.c_uint, vp, vp, vp, C.c_uint,
+                                          C.POINTER(C.c_float), vp]
         L.kg_index_params_default.argtypes = [C.POINTER(IndexParams)]
         L.kg_search_params_default.argtypes = [C.POINTER(SearchParams)]
         _lib = L
@@ -182,6 +199,42 @@ class Context:
         """kg_search_batch_noalloc on device pointers (no device allocation)."""
         self._check(self.L.kg_search_batch_noalloc(self.h, q_ptr, nq, q_stride, C.byref(params), out_ld, ids_ptr,
                                                    d_ptr, c_ptr, cost_ptr))
+
+    def router_train(self, Qtrain, **kw):
+        Qtrain = np.ascontiguousarray(Qtrain, np.float32)
+        p = RouterParams()
+        self.L.kg_router_params_default(C.byref(p))
+        for k, v in kw.items():
+            setattr(p, k, v)
+        info = RouterInfo()
+        self._check(self.L.kg_router_train(self.h, C.byref(p), _ptr(Qtrain), Qtrain.shape[0], Qtrain.strides[0],
+                                           C.byref(info)))
+        return {f: getattr(info, f) for f, _ in RouterInfo._fields_}
+
+    def router_seeds(self, Q, m, out_ld=None):
+        Q = np.ascontiguousarray(Q, np.float32)
+        ld = out_ld or m
+        seeds = np.zeros((Q.shape[0], ld), np.uint32)
+        self._check(self.L.kg_router_seeds(self.h, _ptr(Q), Q.shape[0], Q.strides[0], m, _ptr(seeds), ld))
+        return seeds
+
+    def router_seeds_raw(self, q_ptr, nq, q_stride, m, seeds_ptr, out_ld):
+        """kg_router_seeds on raw (device or host) pointers; returns its device milliseconds."""
+        self._check(self.L.kg_router_seeds(self.h, q_ptr, nq, q_stride, m, seeds_ptr, out_ld))
+        ms = C.c_float()
+        self._check(self.L.kg_last_router_timing(self.h, C.byref(ms)))
+        return ms.value
+
+    def router_gradients(self, d, hidden, clusters, weights, x, labels):
+        x = np.ascontiguousarray(x, np.float32)
+        labels = np.ascontiguousarray(labels, np.int32)
+        w = None if weights is None else np.ascontiguousarray(weights, np.float32)
+        nparam = d * hidden + hidden + hidden * hidden + hidden + hidden * clusters + clusters
+        grads = np.zeros(nparam, np.float32)
+        loss = C.c_float()
+        self._check(self.L.kg_router_gradients(self.h, d, hidden, clusters, _ptr(w), _ptr(x), _ptr(labels),
+                                               x.shape[0], C.byref(loss), _ptr(grads)))
+        return loss.value, grads
 
     def reverse(self, k):
         self._check(self.L.kg_reverse(self.h, k))

@@ -155,6 +155,7 @@ void kg_ctx_destroy(kg_ctx *c) {
                       &c->out_ids, &c->out_d, &c->out_cnt, &c->out_cost};
     for (DevBuf *b : bufs) b->release();
     for (auto &b : c->build_scratch) b.release();
+    kgb::router_release(c->router);
     cudaEventDestroy(c->ev0);
     cudaEventDestroy(c->ev1);
     cudaStreamDestroy(c->stream);

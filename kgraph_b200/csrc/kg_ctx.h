@@ -10,6 +10,9 @@
 
 namespace kgb {
 
+struct RouterState;
+void router_release(RouterState *r);
+
 // A device buffer that only grows.
 struct DevBuf {
     void *p = nullptr;
@@ -42,7 +45,7 @@ struct kg_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::mutex mu;
     std::string err;
-    float last_build_ms = 0.f, last_search_ms = 0.f;
+    float last_build_ms = 0.f, last_search_ms = 0.f, last_router_ms = 0.f;
     unsigned long long last_work[2] = {0, 0};
 
     // dataset
@@ -70,6 +73,7 @@ struct kg_ctx {
     std::vector<uint32_t> h_stage_u32;
 
     kgb::DevBuf build_scratch[24];   // NN-descent state (kg_build.cu)
+    kgb::RouterState *router = nullptr;   // learned entry router (kg_router.cu)
 };
 
 namespace kgb {

@@ -1,0 +1,701 @@
+// Learned entry router: predicts, for a query, the graph regions its walk
+// should start from, and hands them to the search as the reference's own
+// user-provided starting points (SearchParams::init with ids as input,
+// kgraph.cpp:461-467; doc/params.md "User-Provided Starting Points").
+//
+// Why.  The reference seeds every query with the same P random nodes
+// (kgraph.cpp:444-453).  On clustered data the k-NN graph splits into one
+// component per cluster, so plain search needs P large enough that some seed
+// falls in the query's cluster (P ~ 1000 for 256 clusters at 1M points).  A
+// seed inside the right cluster reaches the same neighbours with a pool of
+// P ~ 50..100.
+//
+// What runs on the GPU, all in this file:
+//   * entry clusters: k-means (C clusters) of the dataset -- assignment by a
+//     BF16 x BF16 -> FP32 tiled GEMM against the centroids plus an argmin, update
+//     by atomics; per cluster the member nearest its centroid is the entry node;
+//   * the MLP  D -> H -> H -> C  (ReLU), BF16 weights with FP32 master copies,
+//     FP32 accumulation: forward, softmax cross-entropy, backward and Adam, every
+//     step by the kernels below;
+//   * training pairs: (query, cluster of the best node the plain search finds);
+//   * inference: top-m clusters per query -> their entry nodes.
+#include <cuda_bf16.h>
+#include <algorithm>
+#include <cmath>
+#include <random>
+#include <vector>
+#include "kg_ctx.h"
+
+namespace kgb {
+
+namespace {
+
+constexpr int GT = 64;        // GEMM tile (rows and columns of C per block)
+constexpr int GK = 32;        // K step
+
+// C[M,N] = op(A)[M,K] * op(B)[K,N] (+ bias[N]) (ReLU), FP32 out, optional BF16
+// copy.  op(A) = A (row-major, lda) or A^T (A is K x M, lda); same for B.
+// 256 threads, each 4x4 outputs of a 64x64 tile, operands staged through
+// shared memory as FP32.
+__global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int K, const __nv_bfloat16 *A, int lda, int ta,
+                                                   const __nv_bfloat16 *B, int ldb, int tb, float *C, int ldc,
+                                                   __nv_bfloat16 *Cb, const float *bias, int relu, float beta) {
+    __shared__ float As[GK][GT + 4];
+    __shared__ float Bs[GK][GT + 4];
+    const int tid = threadIdx.x;
+    const int r0 = blockIdx.y * GT, c0 = blockIdx.x * GT;
+    const int tr = (tid / 16) * 4, tc = (tid % 16) * 4;
+    float acc[4][4] = {};
+    for (int k0 = 0; k0 < K; k0 += GK) {
+        for (int e = tid; e < GK * GT; e += 256) {
+            const int kk = e / GT, mm = e % GT;
+            const int r = r0 + mm, k = k0 + kk;
+            float v = 0.f;
+            if (r < M && k < K) v = __bfloat162float(ta ? A[(size_t)k * lda + r] : A[(size_t)r * lda + k]);
+            As[kk][mm] = v;
+            const int c = c0 + mm;
+            float w = 0.f;
+            if (c < N && k < K) w = __bfloat162float(tb ? B[(size_t)c * ldb + k] : B[(size_t)k * ldb + c]);
+            Bs[kk][mm] = w;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int kk = 0; kk < GK; ++kk) {
+            float a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) { a[i] = As[kk][tr + i]; b[i] = Bs[kk][tc + i]; }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = __fmaf_rn(a[i], b[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int r = r0 + tr + i;
+        if (r >= M) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int c = c0 + tc + j;
+            if (c >= N) continue;
+            float v = acc[i][j];
+            if (beta != 0.f) v += beta * C[(size_t)r * ldc + c];
+            if (bias) v += bias[c];
+            if (relu) v = fmaxf(v, 0.f);
+            C[(size_t)r * ldc + c] = v;
+            if (Cb) Cb[(size_t)r * ldc + c] = __float2bfloat16_rn(v);
+        }
+    }
+}
+
+__global__ void to_bf16_kernel(const float *x, __nv_bfloat16 *y, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        y[i] = __float2bfloat16_rn(x[i]);
+}
+
+// Rows of the dataset (ld-strided) -> normalised BF16 features (x - mean) * inv_std.
+__global__ void features_kernel(const float *X, uint32_t ld, const uint32_t *rows, uint32_t n, uint32_t d,
+                                const float *mean, const float *inv_std, __nv_bfloat16 *out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (size_t)n * d;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t r = (uint32_t)(i / d), c = (uint32_t)(i % d);
+        const uint32_t row = rows ? rows[r] : r;
+        out[i] = __float2bfloat16_rn((X[(size_t)row * ld + c] - mean[c]) * inv_std[c]);
+    }
+}
+
+// Softmax cross-entropy, one warp per row: loss (summed into *loss), argmax
+// hits (summed into *hits), and dZ = (softmax - onehot) / B as FP32 and BF16.
+__global__ void softmax_ce_kernel(const float *Z, const int32_t *y, int B, int C, float *dZ, __nv_bfloat16 *dZb,
+                                  float *loss, unsigned *hits) {
+    const int lane = threadIdx.x & 31;
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (row >= B) return;
+    const float *z = Z + (size_t)row * C;
+    float mx = -INFINITY;
+    int am = 0;
+    for (int c = lane; c < C; c += 32)
+        if (z[c] > mx) { mx = z[c]; am = c; }
+    for (int o = 16; o; o >>= 1) {
+        const float om = __shfl_xor_sync(0xFFFFFFFFu, mx, o);
+        const int oa = __shfl_xor_sync(0xFFFFFFFFu, am, o);
+        if (om > mx || (om == mx && oa < am)) { mx = om; am = oa; }
+    }
+    float s = 0.f;
+    for (int c = lane; c < C; c += 32) s += expf(z[c] - mx);
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
+    const int t = y[row];
+    if (lane == 0) {
+        atomicAdd(loss, logf(s) + mx - z[t]);
+        if (am == t) atomicAdd(hits, 1u);
+    }
+    if (dZ) {
+        const float inv = 1.f / s, sc = 1.f / B;
+        for (int c = lane; c < C; c += 32) {
+            const float g = (expf(z[c] - mx) * inv - (c == t ? 1.f : 0.f)) * sc;
+            dZ[(size_t)row * C + c] = g;
+            dZb[(size_t)row * C + c] = __float2bfloat16_rn(g);
+        }
+    }
+}
+
+// dH *= (H > 0): the ReLU derivative, FP32 in place plus the BF16 copy.
+__global__ void relu_grad_kernel(float *dH, const float *H, __nv_bfloat16 *dHb, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float g = H[i] > 0.f ? dH[i] : 0.f;
+        dH[i] = g;
+        dHb[i] = __float2bfloat16_rn(g);
+    }
+}
+
+// db[c] = sum over rows of dZ[r, c].
+__global__ void colsum_kernel(const float *dZ, int B, int C, float *db) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C) return;
+    float s = 0.f;
+    for (int r = 0; r < B; ++r) s += dZ[(size_t)r * C + c];
+    db[c] = s;
+}
+
+// Adam (Kingma & Ba 2015) on FP32 master weights, then the BF16 copy.
+__global__ void adam_kernel(float *w, const float *g, float *m, float *v, __nv_bfloat16 *wb, size_t n, float lr,
+                            float b1, float b2, float c1, float c2, float eps) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        w[i] = wi;
+        if (wb) wb[i] = __float2bfloat16_rn(wi);
+    }
+}
+
+// k-means assignment from the GEMM's X.C^T block: argmin_c |c|^2 - 2 x.c.
+__global__ void argmin_kernel(const float *G, const float *cn, int rows, int C, int32_t *lab, float *best) {
+    const int lane = threadIdx.x & 31;
+    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (r >= rows) return;
+    float bv = INFINITY;
+    int bi = 0;
+    for (int c = lane; c < C; c += 32) {
+        const float v = cn[c] - 2.f * G[(size_t)r * C + c];
+        if (v < bv) { bv = v; bi = c; }
+    }
+    for (int o = 16; o; o >>= 1) {
+        const float ov = __shfl_xor_sync(0xFFFFFFFFu, bv, o);
+        const int oi = __shfl_xor_sync(0xFFFFFFFFu, bi, o);
+        if (ov < bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+    }
+    if (lane == 0) { lab[r] = bi; if (best) best[r] = bv; }
+}
+
+// Sums the members of every cluster (features as FP32) and counts them.
+__global__ void kmeans_accumulate_kernel(const __nv_bfloat16 *F, const int32_t *lab, uint32_t n, uint32_t d,
+                                         float *sum, uint32_t *cnt) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (size_t)n * d;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t r = (uint32_t)(i / d), c = (uint32_t)(i % d);
+        atomicAdd(sum + (size_t)lab[r] * d + c, __bfloat162float(F[i]));
+        if (c == 0) atomicAdd(cnt + lab[r], 1u);
+    }
+}
+
+// New centroids = means; an empty cluster keeps its old centroid.  Also |c|^2.
+__global__ void kmeans_update_kernel(float *cent, const float *sum, const uint32_t *cnt, uint32_t C, uint32_t d,
+                                     __nv_bfloat16 *centb, float *cn) {
+    const uint32_t c = blockIdx.x;
+    if (c >= C) return;
+    __shared__ float red[32];
+    float s2 = 0.f;
+    for (uint32_t j = threadIdx.x; j < d; j += blockDim.x) {
+        float v = cent[(size_t)c * d + j];
+        if (cnt[c]) v = sum[(size_t)c * d + j] / cnt[c];
+        const __nv_bfloat16 b = __float2bfloat16_rn(v);
+        cent[(size_t)c * d + j] = v;
+        centb[(size_t)c * d + j] = b;
+        const float bf = __bfloat162float(b);
+        s2 += bf * bf;
+    }
+    for (int o = 16; o; o >>= 1) s2 += __shfl_xor_sync(0xFFFFFFFFu, s2, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.f;
+        for (uint32_t w = 0; w < blockDim.x / 32; ++w) t += red[w];
+        cn[c] = t;
+    }
+}
+
+// Entry node of every cluster: the member nearest its centroid, smallest id on ties.
+__global__ void entry_kernel(const int32_t *lab, const float *best, uint32_t n, unsigned long long *key) {
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        float b = best[r];
+        uint32_t u = __float_as_uint(b);
+        u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);   // order-preserving float key
+        atomicMin(key + lab[r], ((unsigned long long)u << 32) | r);
+    }
+}
+
+// Top-m logits of every row -> entry nodes, in descending logit order.
+__global__ void topm_kernel(const float *Z, int rows, int C, int m, const uint32_t *entry, uint32_t *out, int out_ld) {
+    const int lane = threadIdx.x & 31;
+    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (r >= rows) return;
+    const float *z = Z + (size_t)r * C;
+    unsigned long long taken[4] = {0, 0, 0, 0};   // bitset over lanes' slots: C <= 32 * 64
+    for (int t = 0; t < m; ++t) {
+        float bv = -INFINITY;
+        int bi = -1;
+        for (int c = lane, s = 0; c < C; c += 32, ++s) {
+            if ((taken[s >> 6] >> (s & 63)) & 1ull) continue;
+            if (z[c] > bv) { bv = z[c]; bi = c; }
+        }
+        for (int o = 16; o; o >>= 1) {
+            const float ov = __shfl_xor_sync(0xFFFFFFFFu, bv, o);
+            const int oi = __shfl_xor_sync(0xFFFFFFFFu, bi, o);
+            if (ov > bv || (ov == bv && oi >= 0 && (bi < 0 || oi < bi))) { bv = ov; bi = oi; }
+        }
+        if (bi < 0) bi = 0;
+        if ((bi & 31) == lane) { const int s = bi >> 5; taken[s >> 6] |= 1ull << (s & 63); }
+        if (lane == 0) out[(size_t)r * out_ld + t] = entry[bi];
+    }
+}
+
+void gemm(cudaStream_t st, int M, int N, int K, const __nv_bfloat16 *A, int lda, int ta, const __nv_bfloat16 *B,
+          int ldb, int tb, float *C, int ldc, __nv_bfloat16 *Cb, const float *bias, int relu, float beta = 0.f) {
+    dim3 grid((N + GT - 1) / GT, (M + GT - 1) / GT);
+    gemm_kernel<<<grid, 256, 0, st>>>(M, N, K, A, lda, ta, B, ldb, tb, C, ldc, Cb, bias, relu, beta);
+}
+
+int blocks_for(size_t n, int per = 256) { return (int)std::min<size_t>((n + per - 1) / per, 148 * 32); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Router state (device): weights, Adam moments, activations for one batch.
+struct RouterState {
+    uint32_t D = 0, H = 0, C = 0, batch = 0;
+    bool trained = false;
+    DevBuf mean, inv_std, entry;                 // normalisation, entry node per cluster
+    DevBuf w[3], b[3], wb[3], gw[3], gb[3], mw[3], vw[3], mb[3], vb[3];
+    DevBuf X, H1, H1b, H2, H2b, Z, dZ, dZb, dH, dHb, lab, scal;
+    void release() {
+        DevBuf *all[] = {&mean, &inv_std, &entry, &X, &H1, &H1b, &H2, &H2b, &Z, &dZ, &dZb, &dH, &dHb, &lab, &scal};
+        for (DevBuf *p : all) p->release();
+        for (int l = 0; l < 3; ++l) {
+            DevBuf *ps[] = {&w[l], &b[l], &wb[l], &gw[l], &gb[l], &mw[l], &vw[l], &mb[l], &vb[l]};
+            for (DevBuf *p : ps) p->release();
+        }
+    }
+};
+
+void router_release(RouterState *r) {
+    if (r) { r->release(); delete r; }
+}
+
+namespace {
+
+cudaError_t alloc_router(RouterState &r, uint32_t batch) {
+    const uint32_t in[3] = {r.D, r.H, r.H}, out[3] = {r.H, r.H, r.C};
+    cudaError_t e;
+    for (int l = 0; l < 3; ++l) {
+        const size_t nw = (size_t)in[l] * out[l];
+        DevBuf *f32[] = {&r.w[l], &r.gw[l], &r.mw[l], &r.vw[l]};
+        for (DevBuf *p : f32)
+            if ((e = p->reserve(nw * 4)) != cudaSuccess) return e;
+        if ((e = r.wb[l].reserve(nw * 2)) != cudaSuccess) return e;
+        DevBuf *bs[] = {&r.b[l], &r.gb[l], &r.mb[l], &r.vb[l]};
+        for (DevBuf *p : bs)
+            if ((e = p->reserve(out[l] * 4)) != cudaSuccess) return e;
+    }
+    const size_t B = batch;
+    if ((e = r.X.reserve(B * r.D * 2)) != cudaSuccess || (e = r.H1.reserve(B * r.H * 4)) != cudaSuccess ||
+        (e = r.H1b.reserve(B * r.H * 2)) != cudaSuccess || (e = r.H2.reserve(B * r.H * 4)) != cudaSuccess ||
+        (e = r.H2b.reserve(B * r.H * 2)) != cudaSuccess || (e = r.Z.reserve(B * r.C * 4)) != cudaSuccess ||
+        (e = r.dZ.reserve(B * std::max(r.C, r.H) * 4)) != cudaSuccess || (e = r.dZb.reserve(B * r.C * 2)) != cudaSuccess ||
+        (e = r.dH.reserve(B * r.H * 4)) != cudaSuccess || (e = r.dHb.reserve(B * r.H * 2)) != cudaSuccess ||
+        (e = r.lab.reserve(B * 4)) != cudaSuccess || (e = r.scal.reserve(64)) != cudaSuccess)
+        return e;
+    r.batch = batch;
+    return cudaSuccess;
+}
+
+// Forward of B rows already in r.X (BF16 features): H1, H2, Z.
+void forward(cudaStream_t st, RouterState &r, int B) {
+    gemm(st, B, r.H, r.D, r.X.as<__nv_bfloat16>(), r.D, 0, r.wb[0].as<__nv_bfloat16>(), r.H, 0, r.H1.as<float>(), r.H,
+         r.H1b.as<__nv_bfloat16>(), r.b[0].as<float>(), 1);
+    gemm(st, B, r.H, r.H, r.H1b.as<__nv_bfloat16>(), r.H, 0, r.wb[1].as<__nv_bfloat16>(), r.H, 0, r.H2.as<float>(), r.H,
+         r.H2b.as<__nv_bfloat16>(), r.b[1].as<float>(), 1);
+    gemm(st, B, r.C, r.H, r.H2b.as<__nv_bfloat16>(), r.H, 0, r.wb[2].as<__nv_bfloat16>(), r.C, 0, r.Z.as<float>(), r.C,
+         nullptr, r.b[2].as<float>(), 0);
+}
+
+// Loss and gradients of B rows with labels in r.lab (after forward).
+void backward(cudaStream_t st, RouterState &r, int B) {
+    float *loss = r.scal.as<float>();
+    unsigned *hits = reinterpret_cast<unsigned *>(r.scal.as<char>() + 4);
+    softmax_ce_kernel<<<(B * 32 + 255) / 256, 256, 0, st>>>(r.Z.as<float>(), r.lab.as<int32_t>(), B, r.C,
+                                                            r.dZ.as<float>(), r.dZb.as<__nv_bfloat16>(), loss, hits);
+    // layer 3: dW3 = H2^T dZ, db3, dH2 = dZ W3^T
+    gemm(st, r.H, r.C, B, r.H2b.as<__nv_bfloat16>(), r.H, 1, r.dZb.as<__nv_bfloat16>(), r.C, 0, r.gw[2].as<float>(), r.C,
+         nullptr, nullptr, 0);
+    colsum_kernel<<<(r.C + 255) / 256, 256, 0, st>>>(r.dZ.as<float>(), B, r.C, r.gb[2].as<float>());
+    gemm(st, B, r.H, r.C, r.dZb.as<__nv_bfloat16>(), r.C, 0, r.wb[2].as<__nv_bfloat16>(), r.C, 1, r.dH.as<float>(), r.H,
+         nullptr, nullptr, 0);
+    relu_grad_kernel<<<blocks_for((size_t)B * r.H), 256, 0, st>>>(r.dH.as<float>(), r.H2.as<float>(),
+                                                                  r.dHb.as<__nv_bfloat16>(), (size_t)B * r.H);
+    // layer 2
+    gemm(st, r.H, r.H, B, r.H1b.as<__nv_bfloat16>(), r.H, 1, r.dHb.as<__nv_bfloat16>(), r.H, 0, r.gw[1].as<float>(), r.H,
+         nullptr, nullptr, 0);
+    colsum_kernel<<<(r.H + 255) / 256, 256, 0, st>>>(r.dH.as<float>(), B, r.H, r.gb[1].as<float>());
+    // dH1 = dH2 W2^T (into r.dZ as scratch: B x H fits), then the ReLU mask
+    gemm(st, B, r.H, r.H, r.dHb.as<__nv_bfloat16>(), r.H, 0, r.wb[1].as<__nv_bfloat16>(), r.H, 1, r.dZ.as<float>(), r.H,
+         nullptr, nullptr, 0);
+    relu_grad_kernel<<<blocks_for((size_t)B * r.H), 256, 0, st>>>(r.dZ.as<float>(), r.H1.as<float>(),
+                                                                  r.dHb.as<__nv_bfloat16>(), (size_t)B * r.H);
+    // layer 1
+    gemm(st, r.D, r.H, B, r.X.as<__nv_bfloat16>(), r.D, 1, r.dHb.as<__nv_bfloat16>(), r.H, 0, r.gw[0].as<float>(), r.H,
+         nullptr, nullptr, 0);
+    colsum_kernel<<<(r.H + 255) / 256, 256, 0, st>>>(r.dZ.as<float>(), B, r.H, r.gb[0].as<float>());
+}
+
+void init_weights(RouterState &r, uint64_t seed) {
+    std::mt19937_64 rng(seed);
+    const uint32_t in[3] = {r.D, r.H, r.H}, out[3] = {r.H, r.H, r.C};
+    for (int l = 0; l < 3; ++l) {
+        const size_t nw = (size_t)in[l] * out[l];
+        std::normal_distribution<float> nd(0.f, std::sqrt(2.f / in[l]));   // He initialisation
+        std::vector<float> h(nw);
+        for (auto &x : h) x = nd(rng);
+        cudaMemcpy(r.w[l].p, h.data(), nw * 4, cudaMemcpyHostToDevice);
+        cudaMemset(r.b[l].p, 0, out[l] * 4);
+        cudaMemset(r.mw[l].p, 0, nw * 4);
+        cudaMemset(r.vw[l].p, 0, nw * 4);
+        cudaMemset(r.mb[l].p, 0, out[l] * 4);
+        cudaMemset(r.vb[l].p, 0, out[l] * 4);
+        to_bf16_kernel<<<blocks_for(nw), 256>>>(r.w[l].as<float>(), r.wb[l].as<__nv_bfloat16>(), nw);
+    }
+}
+
+}  // namespace
+}  // namespace kgb
+
+using namespace kgb;
+
+namespace {
+struct Guard {
+    kg_ctx *c;
+    explicit Guard(kg_ctx *ctx) : c(ctx) { c->mu.lock(); cudaSetDevice(c->device); }
+    ~Guard() { c->mu.unlock(); }
+};
+
+// Normalised BF16 features of host/device query rows into r.X (n <= r.batch).
+int stage_queries(kg_ctx *ctx, RouterState &r, const float *q, size_t n, size_t stride, DevBuf &tmp) {
+    cudaError_t e;
+    if ((e = tmp.reserve(n * r.D * 4)) != cudaSuccess) return cuda_fail(ctx, e, "router alloc");
+    e = cudaMemcpy2DAsync(tmp.p, r.D * 4, q, stride, r.D * 4, n, is_device_ptr(q) ? cudaMemcpyDeviceToDevice
+                                                                                   : cudaMemcpyHostToDevice,
+                          ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "router queries");
+    features_kernel<<<blocks_for(n * r.D), 256, 0, ctx->stream>>>(tmp.as<float>(), r.D, nullptr, (uint32_t)n, r.D,
+                                                                    r.mean.as<float>(), r.inv_std.as<float>(),
+                                                                    r.X.as<__nv_bfloat16>());
+    return KG_OK;
+}
+}  // namespace
+
+extern "C" int kg_last_router_timing(kg_ctx *ctx, float *seeds_ms) {
+    if (!ctx) return KG_E_INVALID;
+    if (seeds_ms) *seeds_ms = ctx->last_router_ms;
+    return KG_OK;
+}
+
+extern "C" void kg_router_params_default(kg_router_params *p) {
+    p->clusters = 1024;
+    p->hidden = 256;
+    p->kmeans_iters = 8;
+    p->label_P = 1000;
+    p->epochs = 4;
+    p->batch = 1024;
+    p->lr = 2e-3f;
+    p->seed = 1998;
+}
+
+extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const float *train_queries, size_t ntrain,
+                               size_t q_stride_bytes, kg_router_info *info) {
+    if (!ctx) return KG_E_INVALID;
+    if (!p || !train_queries || ntrain == 0) return set_error(ctx, KG_E_INVALID, "bad router arguments");
+    {
+        Guard g(ctx);
+        if (!ctx->has_data || !ctx->has_graph) return set_error(ctx, KG_E_RUNTIME, "router needs a dataset and a graph");
+        if (p->clusters < 2 || p->clusters > 2048 || p->hidden < 8 || p->batch < 1)
+            return set_error(ctx, KG_E_INVALID, "router sizes out of range (clusters 2..2048)");
+    }
+    // 1. labels: the best node the plain search finds for each training query
+    std::vector<uint32_t> top(ntrain), cnt(ntrain);
+    {
+        kg_search_params sp;
+        kg_search_params_default(&sp);
+        sp.K = 1;
+        sp.P = p->label_P;
+        int rc = kg_search_batch(ctx, train_queries, ntrain, q_stride_bytes, &sp, nullptr, nullptr, 1, top.data(),
+                                 nullptr, cnt.data(), nullptr);
+        if (rc != KG_OK) return rc;
+    }
+    Guard g(ctx);
+    cudaStream_t st = ctx->stream;
+    cudaError_t e;
+    if (!ctx->router) ctx->router = new RouterState;
+    RouterState &r = *ctx->router;
+    r.trained = false;
+    r.D = ctx->d;
+    r.H = p->hidden;
+    r.C = p->clusters;
+    const uint32_t N = ctx->n, D = ctx->d, C = r.C;
+    if ((e = alloc_router(r, std::max<uint32_t>(p->batch, 4096))) != cudaSuccess) return cuda_fail(ctx, e, "router alloc");
+    DevBuf &s0 = ctx->build_scratch[20], &s1 = ctx->build_scratch[21], &s2 = ctx->build_scratch[22],
+           &s3 = ctx->build_scratch[23];
+
+    // 2. normalisation over the dataset (per-dimension mean and 1/std)
+    std::vector<float> hX((size_t)N * D);
+    cudaMemcpy2D(hX.data(), D * 4, ctx->X.p, ctx->ld * 4, D * 4, N, cudaMemcpyDeviceToHost);
+    std::vector<double> mu(D, 0.0), var(D, 0.0);
+    for (size_t i = 0; i < (size_t)N * D; ++i) mu[i % D] += hX[i];
+    for (uint32_t j = 0; j < D; ++j) mu[j] /= N;
+    for (size_t i = 0; i < (size_t)N * D; ++i) { double t = hX[i] - mu[i % D]; var[i % D] += t * t; }
+    std::vector<float> hm(D), hs(D);
+    for (uint32_t j = 0; j < D; ++j) { hm[j] = (float)mu[j]; hs[j] = (float)(1.0 / std::sqrt(var[j] / N + 1e-6)); }
+    if ((e = r.mean.reserve(D * 4)) != cudaSuccess || (e = r.inv_std.reserve(D * 4)) != cudaSuccess ||
+        (e = r.entry.reserve(C * 4)) != cudaSuccess)
+        return cuda_fail(ctx, e, "router alloc");
+    cudaMemcpyAsync(r.mean.p, hm.data(), D * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(r.inv_std.p, hs.data(), D * 4, cudaMemcpyHostToDevice, st);
+
+    // 3. k-means of the dataset features: C centroids from random members
+    if ((e = s0.reserve((size_t)N * D * 2)) != cudaSuccess ||            // features (BF16)
+        (e = s1.reserve((size_t)C * D * 4 * 2 + (size_t)C * D * 2 + C * 8)) != cudaSuccess ||   // cent, sum, centb, cn, cnt
+        (e = s2.reserve((size_t)N * 4 * 2)) != cudaSuccess ||              // labels, best
+        (e = s3.reserve((size_t)65536 * C * 4)) != cudaSuccess)            // one block of X.C^T
+        return cuda_fail(ctx, e, "router alloc");
+    __nv_bfloat16 *F = s0.as<__nv_bfloat16>();
+    float *cent = s1.as<float>();
+    float *csum = cent + (size_t)C * D;
+    __nv_bfloat16 *centb = reinterpret_cast<__nv_bfloat16 *>(csum + (size_t)C * D);
+    float *cn = reinterpret_cast<float *>(centb + (size_t)C * D);
+    uint32_t *ccnt = reinterpret_cast<uint32_t *>(cn + C);
+    int32_t *lab = s2.as<int32_t>();
+    float *best = reinterpret_cast<float *>(lab + N);
+    features_kernel<<<blocks_for((size_t)N * D), 256, 0, st>>>(ctx->X.as<float>(), ctx->ld, nullptr, N, D,
+                                                                 r.mean.as<float>(), r.inv_std.as<float>(), F);
+    {
+        std::mt19937 rng(p->seed);
+        std::vector<uint32_t> pick(C);
+        for (uint32_t c = 0; c < C; ++c) pick[c] = rng() % N;
+        std::vector<float> hc((size_t)C * D);
+        for (uint32_t c = 0; c < C; ++c)
+            for (uint32_t j = 0; j < D; ++j) hc[(size_t)c * D + j] = (hX[(size_t)pick[c] * D + j] - hm[j]) * hs[j];
+        cudaMemcpyAsync(cent, hc.data(), (size_t)C * D * 4, cudaMemcpyHostToDevice, st);
+        cudaMemsetAsync(ccnt, 0, C * 4, st);
+        kmeans_update_kernel<<<C, 128, 0, st>>>(cent, csum, ccnt, C, D, centb, cn);
+    }
+    for (uint32_t it = 0; it <= p->kmeans_iters; ++it) {
+        for (uint32_t r0 = 0; r0 < N; r0 += 65536) {
+            const uint32_t rows = std::min<uint32_t>(65536, N - r0);
+            gemm(st, rows, C, D, F + (size_t)r0 * D, D, 0, centb, D, 1, s3.as<float>(), C, nullptr, nullptr, 0);
+            argmin_kernel<<<(rows * 32 + 255) / 256, 256, 0, st>>>(s3.as<float>(), cn, rows, C, lab + r0, best + r0);
+        }
+        if (it == p->kmeans_iters) break;
+        cudaMemsetAsync(csum, 0, (size_t)C * D * 4, st);
+        cudaMemsetAsync(ccnt, 0, C * 4, st);
+        kmeans_accumulate_kernel<<<blocks_for((size_t)N * D), 256, 0, st>>>(F, lab, N, D, csum, ccnt);
+        kmeans_update_kernel<<<C, 128, 0, st>>>(cent, csum, ccnt, C, D, centb, cn);
+    }
+    // entry node per cluster (nearest member; an empty cluster points at node 0)
+    unsigned long long *key = reinterpret_cast<unsigned long long *>(s3.p);
+    cudaMemsetAsync(key, 0xFF, C * 8, st);
+    entry_kernel<<<blocks_for(N), 256, 0, st>>>(lab, best, N, key);
+    std::vector<unsigned long long> hkey(C);
+    std::vector<int32_t> hlab(N);
+    cudaMemcpyAsync(hkey.data(), key, C * 8, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hlab.data(), lab, (size_t)N * 4, cudaMemcpyDeviceToHost, st);
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "router kmeans");
+    std::vector<uint32_t> hentry(C);
+    uint32_t empty = 0;
+    for (uint32_t c = 0; c < C; ++c) {
+        if (hkey[c] == ~0ull) { hentry[c] = 0; ++empty; }
+        else hentry[c] = (uint32_t)(hkey[c] & 0xFFFFFFFFu);
+    }
+    cudaMemcpyAsync(r.entry.p, hentry.data(), C * 4, cudaMemcpyHostToDevice, st);
+
+    // 4. training set: query features and the cluster of each query's best node
+    std::vector<int32_t> ylab(ntrain);
+    for (size_t i = 0; i < ntrain; ++i) ylab[i] = cnt[i] ? hlab[top[i] < N ? top[i] : 0] : 0;
+    std::vector<float> hq(ntrain * D);
+    cudaMemcpy2D(hq.data(), D * 4, train_queries, q_stride_bytes, D * 4, ntrain, cudaMemcpyDefault);
+    init_weights(r, p->seed);
+    const uint32_t B = p->batch;
+    DevBuf &tq = ctx->build_scratch[19];
+    std::vector<uint32_t> order(ntrain);
+    for (size_t i = 0; i < ntrain; ++i) order[i] = (uint32_t)i;
+    std::mt19937 rng(p->seed + 1);
+    std::vector<float> hbatch((size_t)std::max<uint32_t>(B, 1) * D);
+    std::vector<int32_t> hy(std::max<uint32_t>(B, 1));
+    float last_loss = 0.f;
+    unsigned step = 0;
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    const size_t full = ntrain < B ? ntrain : ntrain / B * B;   // the last partial batch is dropped
+    for (uint32_t ep = 0; ep < p->epochs; ++ep) {
+        std::shuffle(order.begin(), order.end(), rng);
+        for (size_t s0i = 0; s0i < full; s0i += B) {
+            const uint32_t bs = (uint32_t)std::min<size_t>(B, full - s0i);
+            for (uint32_t i = 0; i < bs; ++i) {
+                const size_t qi = order[s0i + i];
+                std::copy(hq.begin() + qi * D, hq.begin() + (qi + 1) * D, hbatch.begin() + (size_t)i * D);
+                hy[i] = ylab[qi];
+            }
+            int rc = stage_queries(ctx, r, hbatch.data(), bs, D * 4, tq);
+            if (rc != KG_OK) return rc;
+            cudaMemcpyAsync(r.lab.p, hy.data(), bs * 4, cudaMemcpyHostToDevice, st);
+            cudaMemsetAsync(r.scal.p, 0, 8, st);
+            forward(st, r, bs);
+            backward(st, r, bs);
+            ++step;
+            const float c1 = 1.f - std::pow(b1, (float)step), c2 = 1.f - std::pow(b2, (float)step);
+            const uint32_t in[3] = {r.D, r.H, r.H}, out[3] = {r.H, r.H, r.C};
+            for (int l = 0; l < 3; ++l) {
+                const size_t nw = (size_t)in[l] * out[l];
+                adam_kernel<<<blocks_for(nw), 256, 0, st>>>(r.w[l].as<float>(), r.gw[l].as<float>(), r.mw[l].as<float>(),
+                                                             r.vw[l].as<float>(), r.wb[l].as<__nv_bfloat16>(), nw, p->lr, b1,
+                                                             b2, c1, c2, eps);
+                adam_kernel<<<blocks_for(out[l]), 256, 0, st>>>(r.b[l].as<float>(), r.gb[l].as<float>(),
+                                                                 r.mb[l].as<float>(), r.vb[l].as<float>(), nullptr,
+                                                                 out[l], p->lr, b1, b2, c1, c2, eps);
+            }
+            float hl = 0.f;
+            cudaMemcpyAsync(&hl, r.scal.p, 4, cudaMemcpyDeviceToHost, st);
+            if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "router train");
+            last_loss = hl / bs;
+        }
+    }
+    // accuracy of the final weights on the first min(ntrain, 4096) training rows
+    float acc = 0.f;
+    {
+        const size_t n = std::min<size_t>(ntrain, 4096);
+        unsigned hits_total = 0;
+        for (size_t c0 = 0; c0 < n; c0 += r.batch) {
+            const uint32_t bs = (uint32_t)std::min<size_t>(r.batch, n - c0);
+            int rc = stage_queries(ctx, r, hq.data() + c0 * D, bs, D * 4, tq);
+            if (rc != KG_OK) return rc;
+            cudaMemcpyAsync(r.lab.p, ylab.data() + c0, bs * 4, cudaMemcpyHostToDevice, st);
+            cudaMemsetAsync(r.scal.p, 0, 8, st);
+            forward(st, r, bs);
+            softmax_ce_kernel<<<(bs * 32 + 255) / 256, 256, 0, st>>>(r.Z.as<float>(), r.lab.as<int32_t>(), bs, r.C,
+                                                                     nullptr, nullptr, r.scal.as<float>(),
+                                                                     reinterpret_cast<unsigned *>(r.scal.as<char>() + 4));
+            unsigned h = 0;
+            cudaMemcpyAsync(&h, r.scal.as<char>() + 4, 4, cudaMemcpyDeviceToHost, st);
+            if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "router eval");
+            hits_total += h;
+        }
+        acc = n ? (float)hits_total / n : 0.f;
+    }
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "router train");
+    r.trained = true;
+    if (info) {
+        info->steps = step;
+        info->final_loss = last_loss;
+        info->train_accuracy = acc;
+        info->empty_clusters = empty;
+    }
+    return check_device_error(ctx, "router");
+}
+
+extern "C" int kg_router_seeds(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes, unsigned m,
+                               uint32_t *seeds, size_t out_ld) {
+    if (!ctx) return KG_E_INVALID;
+    Guard g(ctx);
+    if (!ctx->router || !ctx->router->trained) return set_error(ctx, KG_E_RUNTIME, "router not trained");
+    RouterState &r = *ctx->router;
+    if (m == 0 || m > r.C || m > out_ld || m > 64) return set_error(ctx, KG_E_INVALID, "bad number of router seeds");
+    cudaStream_t st = ctx->stream;
+    cudaError_t e;
+    DevBuf &tq = ctx->build_scratch[19], &out = ctx->build_scratch[18];
+    const bool sdev = is_device_ptr(seeds);
+    if (!sdev && (e = out.reserve(nq * out_ld * 4)) != cudaSuccess) return cuda_fail(ctx, e, "router alloc");
+    uint32_t *dst = sdev ? seeds : out.as<uint32_t>();
+    if (!sdev) cudaMemcpyAsync(dst, seeds, nq * out_ld * 4, cudaMemcpyHostToDevice, st);
+    const char *qb = reinterpret_cast<const char *>(queries);
+    cudaEventRecord(ctx->ev0, st);
+    for (size_t c0 = 0; c0 < nq; c0 += r.batch) {
+        const size_t bs = std::min<size_t>(r.batch, nq - c0);
+        int rc = stage_queries(ctx, r, reinterpret_cast<const float *>(qb + c0 * q_stride_bytes), bs, q_stride_bytes, tq);
+        if (rc != KG_OK) return rc;
+        forward(st, r, (int)bs);
+        topm_kernel<<<((int)bs * 32 + 255) / 256, 256, 0, st>>>(r.Z.as<float>(), (int)bs, r.C, (int)m,
+                                                                 r.entry.as<uint32_t>(), dst + c0 * out_ld, (int)out_ld);
+    }
+    cudaEventRecord(ctx->ev1, st);
+    if (!sdev) cudaMemcpyAsync(seeds, dst, nq * out_ld * 4, cudaMemcpyDeviceToHost, st);
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "router seeds");
+    cudaEventElapsedTime(&ctx->last_router_ms, ctx->ev0, ctx->ev1);
+    return KG_OK;
+}
+
+// Loss and gradients of the current weights on n labelled rows (n <= 4096), for
+// checking the kernels against an independent implementation.  weights: if not
+// NULL, W1|b1|W2|b2|W3|b3 (FP32, row-major in x out) replace the router's.
+extern "C" int kg_router_gradients(kg_ctx *ctx, unsigned d, unsigned hidden, unsigned clusters, const float *weights,
+                                   const float *x, const int32_t *labels, unsigned n, float *loss, float *grads) {
+    if (!ctx) return KG_E_INVALID;
+    Guard g(ctx);
+    if (n == 0 || n > 4096) return set_error(ctx, KG_E_INVALID, "n must be in 1..4096");
+    if (!ctx->router) ctx->router = new RouterState;
+    RouterState &r = *ctx->router;
+    cudaStream_t st = ctx->stream;
+    cudaError_t e;
+    if (weights || r.D != d || r.H != hidden || r.C != clusters) {
+        r.D = d; r.H = hidden; r.C = clusters;
+        if ((e = alloc_router(r, 4096)) != cudaSuccess) return cuda_fail(ctx, e, "router alloc");
+        if ((e = r.mean.reserve(d * 4)) != cudaSuccess || (e = r.inv_std.reserve(d * 4)) != cudaSuccess)
+            return cuda_fail(ctx, e, "router alloc");
+        std::vector<float> zero(d, 0.f), one(d, 1.f);
+        cudaMemcpy(r.mean.p, zero.data(), d * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(r.inv_std.p, one.data(), d * 4, cudaMemcpyHostToDevice);
+        r.trained = false;
+    }
+    const uint32_t in[3] = {d, hidden, hidden}, out[3] = {hidden, hidden, clusters};
+    if (weights) {
+        size_t off = 0;
+        for (int l = 0; l < 3; ++l) {
+            const size_t nw = (size_t)in[l] * out[l];
+            cudaMemcpy(r.w[l].p, weights + off, nw * 4, cudaMemcpyHostToDevice);
+            off += nw;
+            cudaMemcpy(r.b[l].p, weights + off, out[l] * 4, cudaMemcpyHostToDevice);
+            off += out[l];
+            to_bf16_kernel<<<blocks_for(nw), 256, 0, st>>>(r.w[l].as<float>(), r.wb[l].as<__nv_bfloat16>(), nw);
+        }
+    }
+    DevBuf &tq = ctx->build_scratch[19];
+    int rc = stage_queries(ctx, r, x, n, (size_t)d * 4, tq);
+    if (rc != KG_OK) return rc;
+    cudaMemcpyAsync(r.lab.p, labels, n * 4, cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(r.scal.p, 0, 8, st);
+    forward(st, r, n);
+    backward(st, r, n);
+    float hl = 0.f;
+    cudaMemcpyAsync(&hl, r.scal.p, 4, cudaMemcpyDeviceToHost, st);
+    size_t off = 0;
+    for (int l = 0; l < 3; ++l) {
+        const size_t nw = (size_t)in[l] * out[l];
+        if (grads) cudaMemcpyAsync(grads + off, r.gw[l].p, nw * 4, cudaMemcpyDeviceToHost, st);
+        off += nw;
+        if (grads) cudaMemcpyAsync(grads + off, r.gb[l].p, out[l] * 4, cudaMemcpyDeviceToHost, st);
+        off += out[l];
+    }
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "router gradients");
+    if (loss) *loss = hl / n;
+    return KG_OK;
+}
