@@ -168,6 +168,39 @@ int kg_router_gradients(kg_ctx *ctx, unsigned d, unsigned hidden, unsigned clust
  * context's stream). */
 int kg_last_router_timing(kg_ctx *ctx, float *seeds_ms);
 
+/* Precision of the NN-descent local join.  No counterpart in the reference
+ * (its join evaluates every pair in FP32, kgraph.cpp:740-751, 797-815).
+ *   KG_JOIN_FP32  every pair's canonical FP32 distance on the CUDA cores;
+ *   KG_JOIN_BF16  the pairs' Gram block on the tensor cores (BF16 operands
+ *                 centred on the node, FP32 accumulation); a pair is skipped
+ *                 only when its BF16 distance minus a rigorous error margin is
+ *                 above both endpoints' radius, every other pair is recomputed
+ *                 in FP32 and inserted exactly as in KG_JOIN_FP32;
+ *                 The BF16 filter runs in the iterations that start with at
+ *                 least half of the pools full (before that every pair passes
+ *                 the radius test and the FP32 join is the cheaper path);
+ *   KG_JOIN_BF16_ALWAYS  the BF16 filter in every iteration;
+ *   KG_JOIN_AUTO  (default) the faster path measured for the build's own
+ *                 workloads: KG_JOIN_FP32 (the join is bound by the locked
+ *                 pool inserts, which the filter does not reduce). */
+enum { KG_JOIN_AUTO = 0, KG_JOIN_FP32 = 1, KG_JOIN_BF16 = 2, KG_JOIN_BF16_ALWAYS = 3 };
+int kg_set_join_precision(kg_ctx *ctx, int mode);
+/* Counters of the last kg_build's join.  mode: KG_JOIN_BF16 when any
+ * iteration ran the tensor-core filter (tc_iterations of them).  pairs: join
+ * pairs (IndexInfo.cost * N(N-1)/2 summed over iterations); rechecked: pairs
+ * recomputed in FP32 after the BF16 filter.  On a sample of nodes every pair
+ * is also evaluated in FP64: sampled pairs, the BF16 tile distance's absolute
+ * and relative error against FP64 (max, mean) and the error as a fraction of
+ * the margin (max, mean; < 1 means the filter was safe); violations = sampled
+ * or rechecked pairs whose error exceeded the margin. */
+typedef struct {
+    int mode;
+    unsigned long long pairs, rechecked, sampled, violations;
+    double max_abs_err, mean_abs_err, max_rel_err, mean_rel_err, max_err_over_margin, mean_err_over_margin;
+    unsigned tc_iterations;
+} kg_join_stats;
+int kg_last_join_stats(kg_ctx *ctx, kg_join_stats *out);
+
 /* Milliseconds of the last kg_build / kg_search_batch device work, measured
  * with CUDA events on the context's stream (for profiling and benchmarks). */
 int kg_last_timing(kg_ctx *ctx, float *build_ms, float *search_ms);

@@ -21,7 +21,10 @@ SYMBOLS = [
     "kg_graph_export", "kg_graph_import", "kg_search_batch", "kg_reverse", "kg_prune", "kg_last_timing",
     "kg_last_search_work", "kg_search_batch_noalloc", "kg_noalloc_scratch_bytes",
     "kg_router_params_default", "kg_router_train", "kg_router_seeds", "kg_router_gradients", "kg_last_router_timing",
+    "kg_set_join_precision", "kg_last_join_stats",
 ]
+
+JOIN = {"auto": 0, "fp32": 1, "bf16": 2, "bf16_always": 3}
 
 
 class IndexParams(C.Structure):
@@ -43,6 +46,14 @@ class RouterParams(C.Structure):
 class RouterInfo(C.Structure):
     _fields_ = [("steps", C.c_uint), ("final_loss", C.c_float), ("train_accuracy", C.c_float),
                 ("empty_clusters", C.c_uint)]
+
+
+class JoinStats(C.Structure):
+    _fields_ = [("mode", C.c_int), ("pairs", C.c_ulonglong), ("rechecked", C.c_ulonglong),
+                ("sampled", C.c_ulonglong), ("violations", C.c_ulonglong), ("max_abs_err", C.c_double),
+                ("mean_abs_err", C.c_double), ("max_rel_err", C.c_double), ("mean_rel_err", C.c_double),
+                ("max_err_over_margin", C.c_double), ("mean_err_over_margin", C.c_double),
+                ("tc_iterations", C.c_uint)]
 
 
 class SearchParams(C.Structure):
@@ -85,6 +96,8 @@ def lib():
         L.kg_router_seeds.argtypes = [vp, vp, sz, sz, C.c_uint, vp, sz]
         L.kg_router_gradients.argtypes = [vp, C.c_uint, C.c_uint, C.c_uint, vp, vp, vp, C.c_uint,
                                           C.POINTER(C.c_float), vp]
+        L.kg_set_join_precision.argtypes = [vp, C.c_int]
+        L.kg_last_join_stats.argtypes = [vp, C.POINTER(JoinStats)]
         L.kg_index_params_default.argtypes = [C.POINTER(IndexParams)]
         L.kg_search_params_default.argtypes = [C.POINTER(SearchParams)]
         _lib = L
@@ -251,6 +264,17 @@ class Context:
         b, s = C.c_float(), C.c_float()
         self._check(self.L.kg_last_timing(self.h, C.byref(b), C.byref(s)))
         return b.value, s.value
+
+    def set_join_precision(self, mode):
+        """'auto' (BF16 tensor-core join for d >= 64), 'fp32', 'bf16' or 'bf16_always'."""
+        self._check(self.L.kg_set_join_precision(self.h, JOIN[mode] if isinstance(mode, str) else int(mode)))
+
+    def join_stats(self):
+        st = JoinStats()
+        self._check(self.L.kg_last_join_stats(self.h, C.byref(st)))
+        out = {f: getattr(st, f) for f, _ in JoinStats._fields_}
+        out["mode"] = {1: "fp32", 2: "bf16"}.get(st.mode, "none")
+        return out
 
 
 def version():

@@ -24,12 +24,14 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstring>
 #include <iostream>
 #include <numeric>
 #include <random>
 #include "kg_build.h"
 #include "kg_ctx.h"
 #include "kg_sort.h"
+#include "kg_insert.cuh"
 #include "kg_warp.cuh"
 
 namespace kgb {
@@ -37,8 +39,6 @@ namespace kgb {
 unsigned g_verbosity = 1;
 
 namespace {
-
-constexpr long long LOCK_LIMIT_CYCLES = 4000000000ll;   // ~2 s at 2 GHz, then an error is reported
 
 // SplitMix64 (Steele, Lea, Flood 2014): one stream per (seed, node, purpose).
 struct Rng {
@@ -138,45 +138,6 @@ __global__ void __launch_bounds__(256) init_kernel(BuildState s) {
 }
 
 // ------------------------------------------------------------------ join
-// Nhood::parallel_try_insert (kgraph.cpp:723-736) by one warp.  Returns the
-// reference's value: pool.size() when the radius test rejects, L+1 for a
-// duplicate, else the insert position.
-__device__ uint32_t locked_insert(const BuildState &s, uint32_t x, uint32_t y, float d, int lane) {
-    float rad = 0.f;
-    if (lane == 0) rad = *reinterpret_cast<volatile float *>(s.radius + x);
-    rad = __shfl_sync(FULL, rad, 0);   // one read, the same decision in every lane
-    if (d > rad) return s.Lp;
-    uint32_t ok = 1;
-    if (lane == 0) {
-        long long t0 = clock64();
-        while (atomicCAS(s.lock + x, 0u, 1u) != 0u) {
-            if (clock64() - t0 > LOCK_LIMIT_CYCLES) { ok = 0; raise_error(s.err, ERR_LOCK_TIMEOUT); break; }
-            __nanosleep(32);
-        }
-    }
-    ok = __shfl_sync(FULL, ok, 0);
-    if (!ok) return s.Lp;
-    __threadfence();
-    volatile float *pd = s.pool_d + (size_t)x * s.PS;
-    volatile uint32_t *pi = s.pool_i + (size_t)x * s.PS;
-    uint32_t Lc = 0;
-    if (lane == 0) Lc = *reinterpret_cast<volatile uint32_t *>(s.nodeL + x);
-    Lc = __shfl_sync(FULL, Lc, 0);
-    uint32_t r = warp_update_knn(pd, pi, (uint32_t *)nullptr, Lc, d, y | FLAG_BIT, 0u, lane);
-    if (r <= Lc) {
-        if (Lc + 1 < s.Lp) {
-            if (lane == 0) *reinterpret_cast<volatile uint32_t *>(s.nodeL + x) = Lc + 1;
-        } else {
-            float nr = pd[Lc - 1];
-            if (lane == 0) *reinterpret_cast<volatile float *>(s.radius + x) = nr;
-        }
-    }
-    __threadfence();
-    __syncwarp();
-    if (lane == 0) atomicExch(s.lock + x, 0u);
-    return r;
-}
-
 // KGraphConstructor::join + Nhood::join (kgraph.cpp:740-751, 797-815).
 __global__ void __launch_bounds__(256) join_kernel(BuildState s) {
     const int lane = threadIdx.x & 31;
@@ -230,22 +191,26 @@ __global__ void __launch_bounds__(256) join_kernel(BuildState s) {
 }
 
 // ------------------------------------------------------------------ statistics
-// Flags in pool[0..K) (EvaluateDelta, kgraph.cpp:148-156) and the sum of M.
+// Flags in pool[0..K) (EvaluateDelta, kgraph.cpp:148-156), the sum of M and
+// the number of full pools.
 __global__ void stats_kernel(BuildState s) {
-    unsigned long long fl = 0, msum = 0;
+    unsigned long long fl = 0, msum = 0, full = 0;
     const uint32_t lim = min(s.K, s.Lp);
     for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < s.D.n; n += gridDim.x * blockDim.x) {
         const uint32_t *pi = s.pool_i + (size_t)n * s.PS;
         for (uint32_t l = 0; l < lim; ++l) fl += (pi[l] & FLAG_BIT) ? 1 : 0;
         msum += s.nodeM[n];
+        full += s.nodeL[n] + 1 >= s.Lp ? 1 : 0;   // pool full: a finite radius
     }
     for (int o = 16; o; o >>= 1) {
         fl += __shfl_xor_sync(FULL, fl, o);
         msum += __shfl_xor_sync(FULL, msum, o);
+        full += __shfl_xor_sync(FULL, full, o);
     }
     if ((threadIdx.x & 31) == 0) {
         atomicAdd(s.stat + 0, fl);
         atomicAdd(s.stat + 1, msum);
+        atomicAdd(s.stat + 2, full);
     }
 }
 
@@ -595,6 +560,27 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
     s.err = ctx->errw.as<uint32_t>();
     cudaStream_t st = ctx->stream;
     cudaMemsetAsync(B[18].p, 0, 64, st);
+    if ((e = ctx->tcstat.reserve(sizeof(JoinTcStats))) != cudaSuccess) return cuda_fail(ctx, e, "alloc build state");
+    s.tc = ctx->tcstat.as<JoinTcStats>();
+    cudaMemsetAsync(s.tc, 0, sizeof(JoinTcStats), st);
+    const bool use_tc = ctx->join_mode == KG_JOIN_BF16 || ctx->join_mode == KG_JOIN_BF16_ALWAYS;
+    if (use_tc && !join_tc_supported(s))
+        return set_error(ctx, KG_E_INVALID, "tensor-core join: lists do not fit in shared memory");
+    JoinQueue jq{};
+    uint64_t *jworst = nullptr, *jpre = nullptr, qcap = 0;
+    if (use_tc) {
+        // (x, y, node) entries for one round's pairs; rounds are cut to fit
+        qcap = std::max<uint64_t>(64ull << 20, 4 * join_tc_node_max(s));
+        if ((e = ctx->joinq.reserve(qcap * 12 + 64)) != cudaSuccess) return cuda_fail(ctx, e, "alloc join queue");
+        if ((e = ctx->joinaux.reserve((n + 1) * 16)) != cudaSuccess) return cuda_fail(ctx, e, "alloc join queue");
+        jq.x = ctx->joinq.as<uint32_t>();
+        jq.y = jq.x + qcap;
+        jq.n = jq.y + qcap;
+        jq.tail = reinterpret_cast<unsigned long long *>(jq.n + qcap + (qcap & 1));
+        jq.work = reinterpret_cast<uint32_t *>(jq.tail + 1);
+        jworst = ctx->joinaux.as<uint64_t>();
+        jpre = jworst + n + 1;
+    }
     cudaMemsetAsync(s.rcnt_new + N, 0, 4, st);   // scan inputs carry one extra zero
     cudaMemsetAsync(s.rcnt_old + N, 0, 4, st);
 
@@ -637,21 +623,52 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
     const float total = N * float(N - 1) / 2;
     std::vector<float> hout((size_t)C * 5);
     unsigned long long hstat[4];
+    unsigned long long fp32_pairs = 0, hstat_prev = 0;
+    double full_frac = 0.0;   // fraction of full pools after the last join
+    unsigned tc_iters = 0;
     for (uint32_t it = 0; (params->iterations <= 0) || (it < params->iterations); ++it) {
         ++inf.iterations;
         s.iteration = it;
         cudaMemsetAsync(s.work, 0, 4, st);
-        join_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
-        cudaMemsetAsync(s.stat, 0, 16, st);
+        // The tensor-core filter can only skip pairs against finite radii: while
+        // most pools are still filling, every pair passes it and the fused
+        // CUDA-core join is the cheaper path.
+        const bool tc_now = use_tc && (ctx->join_mode == KG_JOIN_BF16_ALWAYS || full_frac >= JOIN_TC_MIN_FULL);
+        if (tc_now) {
+            ++tc_iters;
+            // rounds of nodes whose worst-case pair counts fit the queue
+            if ((e = join_tc_worst(st, s, jworst)) != cudaSuccess) return cuda_fail(ctx, e, "join");
+            if ((e = scan_counts64(ctx, jworst, jpre, N)) != cudaSuccess) return cuda_fail(ctx, e, "scan");
+            uint64_t total = 0;
+            cudaMemcpyAsync(&total, jpre + N, 8, cudaMemcpyDeviceToHost, st);
+            if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "join");
+            const uint64_t slab = qcap - join_tc_node_max(s);
+            const uint32_t R = (uint32_t)std::max<uint64_t>(1, (total + slab - 1) / slab);
+            if ((e = ctx->joinb.reserve((size_t)(R + 1) * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc");
+            jq.bounds = ctx->joinb.as<uint32_t>();
+            if ((e = join_tc_bounds(st, jpre, N, slab, R, jq.bounds)) != cudaSuccess) return cuda_fail(ctx, e, "join");
+            for (uint32_t r = 0; r < R; ++r)
+                if ((e = launch_join_tc(ctx->num_sms, grid_for(ctx), st, s, jq, r)) != cudaSuccess)
+                    return cuda_fail(ctx, e, "join");
+        } else {
+            // no shared memory: all of the unified L1 for the pool and row reads
+            cudaFuncSetAttribute(join_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxL1);
+            join_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
+        }
+        cudaMemsetAsync(s.stat, 0, 24, st);
         stats_kernel<<<grid_for(ctx, 4), 256, 0, st>>>(s);
         if (C) controls_kernel<<<(C + 127) / 128, 128, 0, st>>>(s, ctrl, ctrl_d, C, ctrl_out);
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "join");
-        cudaMemcpyAsync(hstat, s.n_comps, 3 * 8, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(hstat, s.n_comps, 4 * 8, cudaMemcpyDeviceToHost, st);
         if (C) cudaMemcpyAsync(hout.data(), ctrl_out, (size_t)C * 5 * 4, cudaMemcpyDeviceToHost, st);
         if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "join");
         int de = check_device_error(ctx, "build");
         if (de != KG_OK) return de;
         // kgraph.cpp:927-963: the per-iteration statistics
+        if (!tc_now) fp32_pairs += hstat[0] - hstat_prev;
+        hstat_prev = hstat[0];
+        full_frac = (double)hstat[3] / N;
         inf.cost = hstat[0] / total;
         inf.delta = (float)((double)hstat[1] / K / N);
         inf.M = (float)((double)hstat[2] / N);
@@ -683,6 +700,10 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
         update_cap_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "update");
     }
+
+    ctx->joinq.release();   // the candidate queue is only needed while joining
+    ctx->joinaux.release();
+    ctx->joinb.release();
 
     // finalize (kgraph.cpp:975-988) into the context's CSR graph
     DevBuf &cnt = ctx->build_scratch[22];
@@ -717,8 +738,39 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
         if (r != KG_OK) return r;
     }
     cudaEventRecord(ctx->ev1, st);
+    JoinTcStats ts{};
+    cudaMemcpyAsync(&ts, s.tc, sizeof(ts), cudaMemcpyDeviceToHost, st);
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "build");
     cudaEventElapsedTime(&ctx->last_build_ms, ctx->ev0, ctx->ev1);
+    kg_join_stats &js = ctx->last_join;
+    js = kg_join_stats{};
+    js.mode = tc_iters ? KG_JOIN_BF16 : KG_JOIN_FP32;
+    js.tc_iterations = tc_iters;
+    js.pairs = hstat_prev;
+    js.rechecked = ts.rechecked + fp32_pairs;
+    js.sampled = ts.sampled;
+    js.violations = ts.violations;
+    auto bits = [](unsigned u) { float f; std::memcpy(&f, &u, 4); return (double)f; };
+    js.max_abs_err = bits(ts.max_abs_bits);
+    js.max_rel_err = bits(ts.max_rel_bits);
+    js.max_err_over_margin = bits(ts.max_ratio_bits);
+    js.mean_abs_err = ts.sampled ? ts.sum_abs / ts.sampled : 0.0;
+    js.mean_err_over_margin = ts.sampled ? ts.sum_ratio / ts.sampled : 0.0;
+    js.mean_rel_err = ts.rel_count ? ts.sum_rel / ts.rel_count : 0.0;
     if (info) *info = inf;
+    return KG_OK;
+}
+
+extern "C" int kg_set_join_precision(kg_ctx *ctx, int mode) {
+    if (!ctx || mode < KG_JOIN_AUTO || mode > KG_JOIN_BF16_ALWAYS) return KG_E_INVALID;
+    std::lock_guard<std::mutex> guard(ctx->mu);
+    ctx->join_mode = mode;
+    return KG_OK;
+}
+
+extern "C" int kg_last_join_stats(kg_ctx *ctx, kg_join_stats *out) {
+    if (!ctx || !out) return KG_E_INVALID;
+    std::lock_guard<std::mutex> guard(ctx->mu);
+    *out = ctx->last_join;
     return KG_OK;
 }

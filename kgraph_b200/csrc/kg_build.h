@@ -30,6 +30,45 @@ struct BuildState {
     uint32_t *work;                      // dynamic work counter
     uint64_t seed;
     uint32_t iteration;
+    struct JoinTcStats *tc;              // tensor-core join counters (kg_join_tc.cu)
 };
+
+// Counters of the tensor-core join, accumulated over a build.  Errors are of
+// the BF16 tile distance against an FP64 evaluation of the same pair, on a
+// sample of nodes; `violations` counts pairs whose tile error exceeded the
+// recheck margin (sampled pairs and rechecked pairs).
+struct JoinTcStats {
+    unsigned long long pairs, rechecked, sampled, violations, rel_count;
+    double sum_abs, sum_ratio, sum_rel;
+    unsigned int max_abs_bits, max_ratio_bits, max_rel_bits, pad;
+};
+
+// Candidate pairs between the two phases of a tensor-core join round.  A
+// round covers the nodes [bounds[r], bounds[r+1]), chosen from prefix sums of
+// each node's worst-case pair count so that the round's pairs fit the queue.
+struct JoinQueue {
+    uint32_t *x, *y, *n;
+    unsigned long long *tail;
+    uint32_t *work;      // claim counter within a round
+    uint32_t *bounds;    // round boundaries (node ids)
+};
+constexpr int JOIN_TC_MAX_CTAS_PER_SM = 3;
+// Fraction of full pools (finite radii) from which an iteration's join runs
+// on the tensor cores.
+constexpr double JOIN_TC_MIN_FULL = 0.5;
+
+// One round of the tensor-core local join (kg_join_tc.cu): the filter over the
+// round's nodes, then the inserts of the queued pairs.
+cudaError_t launch_join_tc(int num_sms, int grid_insert, cudaStream_t st, const BuildState &s, JoinQueue jq,
+                           uint32_t round);
+// worst[n] = node n's largest pair count (n < N), worst[N] = 0.
+cudaError_t join_tc_worst(cudaStream_t st, const BuildState &s, uint64_t *worst);
+// bounds[0..R] from the exclusive prefix `pre` of worst (R rounds of <= slab).
+cudaError_t join_tc_bounds(cudaStream_t st, const uint64_t *pre, uint32_t N, uint64_t slab, uint32_t R,
+                           uint32_t *bounds);
+// Whether the tensor-core join supports this state (shared memory fits).
+bool join_tc_supported(const BuildState &s);
+// Largest number of join pairs one node can produce.
+uint64_t join_tc_node_max(const BuildState &s);
 
 }  // namespace kgb

@@ -40,6 +40,7 @@ enum : uint32_t {
     ERR_BAD_ID = 1u << 2,         // an id >= n was met (corrupt graph / init ids)
     ERR_INIT_K = 1u << 3,         // init >= K for a query (reference: invalid_argument)
     ERR_STEP_LIMIT = 1u << 4,     // a search walk exceeded its step bound (never expected)
+    ERR_TC_TIMEOUT = 1u << 5,     // a tensor-core completion wait ran out of cycles
 };
 
 constexpr uint32_t FLAG_BIT = 0x80000000u;

@@ -44,6 +44,7 @@ int check_device_error(kg_ctx *ctx, const char *what) {
     if (w & ERR_CAPACITY) m += " list capacity exceeded;";
     if (w & ERR_BAD_ID) m += " node id out of range;";
     if (w & ERR_STEP_LIMIT) m += " search step bound exceeded;";
+    if (w & ERR_TC_TIMEOUT) m += " tensor-core completion wait limit reached;";
     if (w & ERR_INIT_K) { return set_error(ctx, KG_E_INVALID, "L < params.K"); }
     return set_error(ctx, KG_E_DEVICE, m);
 }
@@ -152,7 +153,7 @@ void kg_ctx_destroy(kg_ctx *c) {
     cudaStreamSynchronize(c->stream);
     DevBuf *bufs[] = {&c->X, &c->norms, &c->offsets, &c->nbr, &c->nbr_d, &c->Mnode, &c->errw, &c->counter, &c->ell, &c->meta,
                       &c->visited, &c->qbuf, &c->kbuf, &c->pbuf, &c->seeds, &c->seed_index, &c->init_ids,
-                      &c->out_ids, &c->out_d, &c->out_cnt, &c->out_cost};
+                      &c->out_ids, &c->out_d, &c->out_cnt, &c->out_cost, &c->tcstat, &c->joinq, &c->joinaux, &c->joinb};
     for (DevBuf *b : bufs) b->release();
     for (auto &b : c->build_scratch) b.release();
     kgb::router_release(c->router);

@@ -73,6 +73,10 @@ struct kg_ctx {
     std::vector<uint32_t> h_stage_u32;
 
     kgb::DevBuf build_scratch[24];   // NN-descent state (kg_build.cu)
+    int join_mode = KG_JOIN_AUTO;
+    kgb::DevBuf tcstat;              // tensor-core join counters
+    kgb::DevBuf joinq, joinaux, joinb;   // tensor-core join: candidate queue, worst-case prefix, round bounds
+    kg_join_stats last_join{};
     kgb::RouterState *router = nullptr;   // learned entry router (kg_router.cu)
 };
 
