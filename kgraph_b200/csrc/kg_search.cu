@@ -143,6 +143,13 @@ __device__ __forceinline__ float warp_cand_dist(const SearchArgs &a, const float
     return mine;
 }
 
+// Hint: bring dataset row `id` into L2 (four 128-byte lines for D = 128).
+__device__ __forceinline__ void prefetch_row(const DataView &D, uint32_t id) {
+    const char *p = reinterpret_cast<const char *>(D.X + (size_t)id * D.ld);
+    const uint32_t bytes = D.ld * 4;
+    for (uint32_t o = 0; o < bytes; o += 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(p + o));
+}
+
 __device__ __forceinline__ bool visited_test_set(uint32_t *vis, uint32_t id) {
     uint32_t bit = 1u << (id & 31);
     uint32_t old = atomicOr(vis + (id >> 5), bit);
@@ -151,7 +158,7 @@ __device__ __forceinline__ bool visited_test_set(uint32_t *vis, uint32_t id) {
 
 }  // namespace
 
-__global__ void __launch_bounds__(256) search_kernel(SearchArgs a) {
+__global__ void __launch_bounds__(256, 4) search_kernel(SearchArgs a) {
     extern __shared__ __align__(16) char smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -334,6 +341,14 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a) {
                             if ((uint32_t)cc == c) { id = wid[cc]; uv = wuv[cc]; }
                         const bool cand = uv && (uint32_t)lane >= lo && (uint32_t)lane < hi;
                         const unsigned cm = __ballot_sync(FULL, cand);
+                        // L2 prefetch of the rows the next two batches of this entry will
+                        // read (unvisited window ids), behind this batch's loads
+#pragma unroll
+                        for (int cc = 0; cc < 4; ++cc) {
+                            const uint32_t pos = wlo + 32 * cc + lane;
+                            if (wuv[cc] && pos >= p1 && pos < p1 + 2 * S && pos < whi)
+                                prefetch_row(a.D, wid[cc]);
+                        }
                         if (cm) {
                             // All three in flight together: the exact test-and-set of the
                             // visited bit, the candidate's {M, degree}, and its row (distance).
