@@ -204,6 +204,11 @@ int kg_last_join_stats(kg_ctx *ctx, kg_join_stats *out);
 /* Milliseconds of the last kg_build / kg_search_batch device work, measured
  * with CUDA events on the context's stream (for profiling and benchmarks). */
 int kg_last_timing(kg_ctx *ctx, float *build_ms, float *search_ms);
+/* CUDA graph launches of the last kg_build's iterations.  No counterpart in
+ * the reference: each NN-descent iteration (update, join, statistics) is
+ * captured once and replayed as one graph launch (two with the statistics
+ * split off when the join runs on the tensor cores, three with its update). */
+int kg_last_build_graphs(kg_ctx *ctx, unsigned *graph_launches);
 /* Work of the last kg_search_batch: distance evaluations (seeds included;
  * the sum of SearchInfo.cost * N plus the seeds) and adjacency entries read. */
 int kg_last_search_work(kg_ctx *ctx, uint64_t *evaluations, uint64_t *adjacency_reads);

@@ -21,7 +21,7 @@ SYMBOLS = [
     "kg_graph_export", "kg_graph_import", "kg_search_batch", "kg_reverse", "kg_prune", "kg_last_timing",
     "kg_last_search_work", "kg_search_batch_noalloc", "kg_noalloc_scratch_bytes",
     "kg_router_params_default", "kg_router_train", "kg_router_seeds", "kg_router_gradients", "kg_last_router_timing",
-    "kg_set_join_precision", "kg_last_join_stats",
+    "kg_set_join_precision", "kg_last_join_stats", "kg_last_build_graphs",
 ]
 
 JOIN = {"auto": 0, "fp32": 1, "bf16": 2, "bf16_always": 3}
@@ -98,6 +98,7 @@ def lib():
                                           C.POINTER(C.c_float), vp]
         L.kg_set_join_precision.argtypes = [vp, C.c_int]
         L.kg_last_join_stats.argtypes = [vp, C.POINTER(JoinStats)]
+        L.kg_last_build_graphs.argtypes = [vp, C.POINTER(C.c_uint)]
         L.kg_index_params_default.argtypes = [C.POINTER(IndexParams)]
         L.kg_search_params_default.argtypes = [C.POINTER(SearchParams)]
         _lib = L
@@ -275,6 +276,12 @@ class Context:
         out = {f: getattr(st, f) for f, _ in JoinStats._fields_}
         out["mode"] = {1: "fp32", 2: "bf16"}.get(st.mode, "none")
         return out
+
+    def build_graph_launches(self):
+        """CUDA graph launches of the last build's iterations."""
+        v = C.c_uint()
+        self._check(self.L.kg_last_build_graphs(self.h, C.byref(v)))
+        return v.value
 
 
 def version():

@@ -93,6 +93,37 @@ struct GPoolAcc {   // gnu_sort over one pool row (dist, id) in global memory
 __device__ __forceinline__ uint32_t warp_id_global() { return (blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
 __device__ __forceinline__ uint32_t warps_total() { return (gridDim.x * blockDim.x) >> 5; }
 
+// Pinned host memory released on scope exit.
+struct HostPinned {
+    char *p = nullptr;
+    cudaError_t alloc(size_t b) { return cudaMallocHost(reinterpret_cast<void **>(&p), b); }
+    ~HostPinned() { if (p) cudaFreeHost(p); }
+};
+
+// A stream capture, instantiated once and replayed; released on scope exit.
+struct StreamGraph {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t x = nullptr;
+    StreamGraph() = default;
+    StreamGraph(const StreamGraph &) = delete;
+    StreamGraph &operator=(const StreamGraph &) = delete;
+    ~StreamGraph() {
+        if (x) cudaGraphExecDestroy(x);
+        if (g) cudaGraphDestroy(g);
+    }
+    bool ready() const { return x != nullptr; }
+    template <class F> cudaError_t capture(cudaStream_t st, F &&record) {
+        cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return e;
+        const cudaError_t er = record();
+        const cudaError_t ee = cudaStreamEndCapture(st, &g);
+        if (er != cudaSuccess) return er;
+        if (ee != cudaSuccess) return ee;
+        return cudaGraphInstantiate(&x, g, 0);
+    }
+    cudaError_t launch(cudaStream_t st) const { return cudaGraphLaunch(x, st); }
+};
+
 // ------------------------------------------------------------------ init
 // kgraph.cpp:760-796 for one node per warp.
 __global__ void __launch_bounds__(256) init_kernel(BuildState s) {
@@ -337,7 +368,7 @@ __global__ void update_cap_kernel(BuildState s) {
             if (s.R && c > s.R) {
                 take = s.R;
                 if (lane == 0) {   // partial Fisher-Yates: the first R of a uniform shuffle
-                    Rng rng = make_rng(s.seed, n, 16 + 2 * (uint64_t)s.iteration + kind);
+                    Rng rng = make_rng(s.seed, n, 16 + 2 * (uint64_t)*s.iter + kind);
                     for (uint32_t i = 0; i < take; ++i) {
                         uint32_t j = i + rng.next() % (c - i);
                         uint32_t tmp = src[i]; src[i] = src[j]; src[j] = tmp;
@@ -358,6 +389,11 @@ __global__ void update_cap_kernel(BuildState s) {
             if (lane == 0) *cnt = have + take;
         }
     }
+}
+
+// Ends an update: the next iteration's number (the R-subset streams are keyed by it).
+__global__ void iter_advance_kernel(BuildState s) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) ++*s.iter;
 }
 
 // ------------------------------------------------------------------ finalize
@@ -473,14 +509,15 @@ cudaError_t launch_linear_search(kg_ctx *ctx, const uint32_t *rows, uint32_t C, 
     return cudaGetLastError();
 }
 
-// Exclusive scan of n u32/u64 counts into out[n+1] (CUB).
-cudaError_t scan_counts(kg_ctx *ctx, const uint32_t *in, uint64_t *out, uint32_t n) {
-    DevBuf &tmp = ctx->build_scratch[23];
+// Exclusive scan of n u32/u64 counts into out[n+1] (CUB), with temporary
+// storage in `tmp` (the shared scan buffer unless the caller gives its own).
+cudaError_t scan_counts(kg_ctx *ctx, const uint32_t *in, uint64_t *out, uint32_t n, DevBuf *tmp = nullptr) {
+    if (!tmp) tmp = &ctx->build_scratch[23];
     size_t bytes = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n + 1, ctx->stream);
-    cudaError_t e = tmp.reserve(bytes);
+    cudaError_t e = tmp->reserve(bytes);
     if (e != cudaSuccess) return e;
-    return cub::DeviceScan::ExclusiveSum(tmp.p, bytes, in, out, n + 1, ctx->stream);
+    return cub::DeviceScan::ExclusiveSum(tmp->p, bytes, in, out, n + 1, ctx->stream);
 }
 cudaError_t scan_counts64(kg_ctx *ctx, const uint64_t *in, uint64_t *out, uint32_t n) {
     DevBuf &tmp = ctx->build_scratch[23];
@@ -557,6 +594,7 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
     s.n_comps = B[18].as<unsigned long long>();
     s.stat = s.n_comps + 1;
     s.work = reinterpret_cast<uint32_t *>(s.n_comps + 4);
+    s.iter = s.work + 2;
     s.err = ctx->errw.as<uint32_t>();
     cudaStream_t st = ctx->stream;
     cudaMemsetAsync(B[18].p, 0, 64, st);
@@ -621,27 +659,87 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
     inf.iterations = 0;
     inf.delta = 1.0f;
     const float total = N * float(N - 1) / 2;
-    std::vector<float> hout((size_t)C * 5);
-    unsigned long long hstat[4];
+    // Pinned host copies of each iteration's statistics; the graphs copy into them.
+    HostPinned hp;
+    if ((e = hp.alloc(64 + (size_t)C * 5 * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc host stats");
+    const unsigned long long *hstat = reinterpret_cast<unsigned long long *>(hp.p);
+    const float *hout = reinterpret_cast<float *>(hp.p + 64);
     unsigned long long fp32_pairs = 0, hstat_prev = 0;
     double full_frac = 0.0;   // fraction of full pools after the last join
     unsigned tc_iters = 0;
+
+    // One iteration's device work, recorded into the stream: the FP32 join,
+    // the statistics with their copies to the host, and the update.
+    auto rec_join = [&]() -> cudaError_t {
+        cudaMemsetAsync(s.work, 0, 4, st);
+        join_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
+        return cudaGetLastError();
+    };
+    auto rec_stats = [&]() -> cudaError_t {
+        cudaMemsetAsync(s.stat, 0, 24, st);
+        stats_kernel<<<grid_for(ctx, 4), 256, 0, st>>>(s);
+        if (C) controls_kernel<<<(C + 127) / 128, 128, 0, st>>>(s, ctrl, ctrl_d, C, ctrl_out);
+        cudaMemcpyAsync(hp.p, s.n_comps, 4 * 8, cudaMemcpyDeviceToHost, st);
+        if (C) cudaMemcpyAsync(hp.p + 64, ctrl_out, (size_t)C * 5 * 4, cudaMemcpyDeviceToHost, st);
+        return cudaGetLastError();
+    };
+    DevBuf &gscan = B[24];   // scan storage owned by the captured update (never reallocated under it)
+    auto rec_update = [&]() -> cudaError_t {
+        update_m_kernel<<<grid_for(ctx, 4), 256, 0, st>>>(s);
+        update_count_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
+        cudaError_t e2;
+        if ((e2 = scan_counts(ctx, s.rcnt_new, s.roff_new, N, &gscan)) != cudaSuccess) return e2;
+        if ((e2 = scan_counts(ctx, s.rcnt_old, s.roff_old, N, &gscan)) != cudaSuccess) return e2;
+        cudaMemsetAsync(s.rcnt_new, 0, n * 4, st);
+        cudaMemsetAsync(s.rcnt_old, 0, n * 4, st);
+        update_fill_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
+        update_cap_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
+        iter_advance_kernel<<<1, 32, 0, st>>>(s);
+        return cudaGetLastError();
+    };
+    // Everything a capture needs is set up before it: the join's cache carveout
+    // and the update's scan storage.
+    cudaFuncSetAttribute(join_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxL1);
+    {
+        size_t sb = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, sb, s.rcnt_new, s.roff_new, N + 1, st);
+        if ((e = gscan.reserve(sb)) != cudaSuccess) return cuda_fail(ctx, e, "alloc scan");
+    }
+    // The iterations replay captured CUDA graphs.  An FP32 iteration is one
+    // launch: the previous iteration's update (deferred until the host has read
+    // that iteration's statistics and decided to go on), the join and the
+    // statistics.  An iteration whose join runs on the tensor cores (its round
+    // count is decided on the host) launches the update graph, its join rounds,
+    // then the statistics graph.
+    StreamGraph g_first, g_steady, g_update, g_stats;
+    unsigned graph_launches = 0;
+    bool pending_update = false;   // the last iteration's update is still to run
+    bool stopped = false;
+    auto run_graph = [&](StreamGraph &g, auto &&record) -> cudaError_t {
+        if (!g.ready()) {
+            cudaError_t e2 = g.capture(st, record);
+            if (e2 != cudaSuccess) return e2;
+        }
+        ++graph_launches;
+        return g.launch(st);
+    };
     for (uint32_t it = 0; (params->iterations <= 0) || (it < params->iterations); ++it) {
         ++inf.iterations;
-        s.iteration = it;
-        cudaMemsetAsync(s.work, 0, 4, st);
         // The tensor-core filter can only skip pairs against finite radii: while
         // most pools are still filling, every pair passes it and the fused
         // CUDA-core join is the cheaper path.
         const bool tc_now = use_tc && (ctx->join_mode == KG_JOIN_BF16_ALWAYS || full_frac >= JOIN_TC_MIN_FULL);
         if (tc_now) {
             ++tc_iters;
+            if (pending_update && (e = run_graph(g_update, rec_update)) != cudaSuccess)
+                return cuda_fail(ctx, e, "update graph");
+            cudaMemsetAsync(s.work, 0, 4, st);
             // rounds of nodes whose worst-case pair counts fit the queue
             if ((e = join_tc_worst(st, s, jworst)) != cudaSuccess) return cuda_fail(ctx, e, "join");
             if ((e = scan_counts64(ctx, jworst, jpre, N)) != cudaSuccess) return cuda_fail(ctx, e, "scan");
-            uint64_t total = 0;
-            cudaMemcpyAsync(&total, jpre + N, 8, cudaMemcpyDeviceToHost, st);
+            cudaMemcpyAsync(hp.p + 32, jpre + N, 8, cudaMemcpyDeviceToHost, st);
             if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "join");
+            const uint64_t total = reinterpret_cast<const uint64_t *>(hp.p)[4];
             const uint64_t slab = qcap - join_tc_node_max(s);
             const uint32_t R = (uint32_t)std::max<uint64_t>(1, (total + slab - 1) / slab);
             if ((e = ctx->joinb.reserve((size_t)(R + 1) * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc");
@@ -650,18 +748,22 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
             for (uint32_t r = 0; r < R; ++r)
                 if ((e = launch_join_tc(ctx->num_sms, grid_for(ctx), st, s, jq, r)) != cudaSuccess)
                     return cuda_fail(ctx, e, "join");
+            if ((e = run_graph(g_stats, rec_stats)) != cudaSuccess) return cuda_fail(ctx, e, "statistics graph");
+        } else if (pending_update) {
+            e = run_graph(g_steady, [&]() -> cudaError_t {
+                cudaError_t e2 = rec_update();
+                if (e2 == cudaSuccess) e2 = rec_join();
+                return e2 == cudaSuccess ? rec_stats() : e2;
+            });
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "iteration graph");
         } else {
-            // no shared memory: all of the unified L1 for the pool and row reads
-            cudaFuncSetAttribute(join_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 (int)cudaSharedmemCarveoutMaxL1);
-            join_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
+            e = run_graph(g_first, [&]() -> cudaError_t {
+                cudaError_t e2 = rec_join();
+                return e2 == cudaSuccess ? rec_stats() : e2;
+            });
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "iteration graph");
         }
-        cudaMemsetAsync(s.stat, 0, 24, st);
-        stats_kernel<<<grid_for(ctx, 4), 256, 0, st>>>(s);
-        if (C) controls_kernel<<<(C + 127) / 128, 128, 0, st>>>(s, ctrl, ctrl_d, C, ctrl_out);
-        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "join");
-        cudaMemcpyAsync(hstat, s.n_comps, 4 * 8, cudaMemcpyDeviceToHost, st);
-        if (C) cudaMemcpyAsync(hout.data(), ctrl_out, (size_t)C * 5 * 4, cudaMemcpyDeviceToHost, st);
+        pending_update = false;
         if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "join");
         int de = check_device_error(ctx, "build");
         if (de != KG_OK) return de;
@@ -687,19 +789,16 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
                       << " one-recall: " << (C ? ors / C : 0.f) << " one-ratio: " << (C ? (oa / C) / (oe / C) : 0.f)
                       << std::endl;
         }
-        if (inf.delta <= params->delta) { inf.stop_condition = 1; break; }
-        if (inf.recall >= params->recall) { inf.stop_condition = 2; break; }
-        // update (kgraph.cpp:816-883)
-        update_m_kernel<<<grid_for(ctx, 4), 256, 0, st>>>(s);
-        update_count_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
-        if ((e = scan_counts(ctx, s.rcnt_new, s.roff_new, N)) != cudaSuccess) return cuda_fail(ctx, e, "scan");
-        if ((e = scan_counts(ctx, s.rcnt_old, s.roff_old, N)) != cudaSuccess) return cuda_fail(ctx, e, "scan");
-        cudaMemsetAsync(s.rcnt_new, 0, n * 4, st);
-        cudaMemsetAsync(s.rcnt_old, 0, n * 4, st);
-        update_fill_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
-        update_cap_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
-        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "update");
+        if (inf.delta <= params->delta) { inf.stop_condition = 1; stopped = true; break; }
+        if (inf.recall >= params->recall) { inf.stop_condition = 2; stopped = true; break; }
+        pending_update = true;   // update (kgraph.cpp:816-883), launched with the next iteration
     }
+    // The iteration cap ended the loop: the reference has run the last update
+    // (its M growth and flag clearing reach the finalized graph).
+    if (!stopped && pending_update && (e = run_graph(g_update, rec_update)) != cudaSuccess)
+        return cuda_fail(ctx, e, "update graph");
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "update");
+    ctx->last_build_graph_launches = graph_launches;
 
     ctx->joinq.release();   // the candidate queue is only needed while joining
     ctx->joinaux.release();
@@ -765,6 +864,13 @@ extern "C" int kg_set_join_precision(kg_ctx *ctx, int mode) {
     if (!ctx || mode < KG_JOIN_AUTO || mode > KG_JOIN_BF16_ALWAYS) return KG_E_INVALID;
     std::lock_guard<std::mutex> guard(ctx->mu);
     ctx->join_mode = mode;
+    return KG_OK;
+}
+
+extern "C" int kg_last_build_graphs(kg_ctx *ctx, unsigned *graph_launches) {
+    if (!ctx || !graph_launches) return KG_E_INVALID;
+    std::lock_guard<std::mutex> guard(ctx->mu);
+    *graph_launches = ctx->last_build_graph_launches;
     return KG_OK;
 }
 

@@ -29,7 +29,8 @@ struct BuildState {
     uint32_t *err;
     uint32_t *work;                      // dynamic work counter
     uint64_t seed;
-    uint32_t iteration;
+    uint32_t *iter;                      // iteration number, advanced on the device
+                                         // so that one captured graph serves every iteration
     struct JoinTcStats *tc;              // tensor-core join counters (kg_join_tc.cu)
 };
 

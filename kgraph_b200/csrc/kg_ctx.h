@@ -46,6 +46,7 @@ struct kg_ctx {
     std::mutex mu;
     std::string err;
     float last_build_ms = 0.f, last_search_ms = 0.f, last_router_ms = 0.f;
+    unsigned last_build_graph_launches = 0;   // CUDA graph launches of the last build's iterations
     unsigned long long last_work[2] = {0, 0};
 
     // dataset
@@ -72,7 +73,7 @@ struct kg_ctx {
         out_cnt, out_cost;
     std::vector<uint32_t> h_stage_u32;
 
-    kgb::DevBuf build_scratch[24];   // NN-descent state (kg_build.cu)
+    kgb::DevBuf build_scratch[25];   // NN-descent state (kg_build.cu)
     int join_mode = KG_JOIN_AUTO;
     kgb::DevBuf tcstat;              // tensor-core join counters
     kgb::DevBuf joinq, joinaux, joinb;   // tensor-core join: candidate queue, worst-case prefix, round bounds

@@ -97,8 +97,11 @@ def test_build_info_and_errors(gpu_ctx):
     gpu_ctx.set_data(X, "euclidean")
     info = gpu_ctx.build(K=10, L=30, S=8, iterations=2)
     assert info["iterations"] == 2 and info["stop_condition"] == 0
+    # one captured-graph launch per iteration, plus the last update when the cap ends the loop
+    assert gpu_ctx.build_graph_launches() == 3
     info = gpu_ctx.build(K=10, L=30, S=8, iterations=30, recall=0.9)
     assert info["stop_condition"] in (1, 2) and info["recall"] > 0.5
+    assert gpu_ctx.build_graph_launches() == info["iterations"]
     small = capi.Context(0)
     small.set_data(X[:10], "euclidean")
     with pytest.raises(capi.KGError, match="K larger than dataset size"):
