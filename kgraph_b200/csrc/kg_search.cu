@@ -361,10 +361,16 @@ __global__ void __launch_bounds__(256, 4) search_kernel(SearchArgs a) {
                             }
                             const float dd = warp_cand_dist(a, s.q, qn, cm, cand, id, lane);
                             const unsigned nm = __ballot_sync(FULL, isnew);
-                            if (nm) {
-                                n_comps += __popc(nm);
+                            n_comps += __popc(nm);
+                            // A full pool takes a candidate only below its last entry: one at or
+                            // above it lands in the spare slot (kgraph.cpp:503-506), and so does
+                            // every later candidate of the batch that is not closer than it, so
+                            // leaving those out of the merge changes no position.
+                            const unsigned im =
+                                L == cap - 1 ? __ballot_sync(FULL, isnew && dd < s.pd[L - 1]) : nm;
+                            if (im) {
                                 uint32_t mr;   // new entries: flag set, m = 0, M = actual_M
-                                L = warp_batch_insert(s.pd, s.pid, s.pm, L, cap, nm, dd, id | FLAG_BIT, aM << 16,
+                                L = warp_batch_insert(s.pd, s.pid, s.pm, L, cap, im, dd, id | FLAG_BIT, aM << 16,
                                                       &mr, lane);
                                 if (mr <= k) moved = true;   // the expanded entry is no longer at k
                                 if (mr < k) k = mr;
