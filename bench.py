@@ -488,6 +488,8 @@ def main():
             break
     ids100, _, _, _ = ctx.search(Q, K=100, P=max(P_star, 100))
     recall100 = recall_at(ids100, Xt, Qt, gt_d, 100, torch)
+    # launch shape of the search kernel picked by the library's autotuner on a sample
+    tune_plain = ctx.search_autotune(Q[:2000], K=10, P=P_star)
     Xt2 = Xt
 
     # device-resident timing (value)
@@ -559,6 +561,7 @@ def main():
                 break
         if P_r is not None:
             rparams = capi.SearchParams(10, 0, P_r, 10, 1, 1e30, 1998, ROUTER_SEEDS)
+            tune_router = ctx.search_autotune(Q, K=10, P=P_r, init=ROUTER_SEEDS, init_ids=seeds)
 
             def step_router():
                 ms_r = ctx.router_seeds_raw(capi._ptr(q_dev), N_QUERIES, q_dev.stride(0) * 4, ROUTER_SEEDS,
@@ -596,6 +599,7 @@ def main():
                       "recall@10": r_ladder[P_r], "recall_ladder": r_ladder, "ms_per_step": sum(r_ms) / args.steps,
                       "e2e": r_e2e, "train_s": router_train_s, "train": rinfo,
                       "speedup_vs_plain": r_value / value, "search_ms_per_step": sum(r_search_ms) / args.steps,
+                      "autotune": tune_router,
                       "algorithmic_bytes_per_launch": int(r_evals * (DIM * 4 + 4) + r_adj * 4)}
         else:
             router = {"unavailable": "recall target not reached on the router ladder", "recall_ladder": r_ladder,
@@ -630,7 +634,7 @@ def main():
             cpu = {"error": str(e)[:200]}
 
     if rank == 0:
-        plain = {"value": value, "P": P_star, "recall@10": ladder[P_star], "e2e": e2e,
+        plain = {"value": value, "P": P_star, "recall@10": ladder[P_star], "e2e": e2e, "autotune": tune_plain,
                  "ms_per_step": tot_ms_max / args.steps,
                  "roofline": {"achieved": achieved, "frac": achieved / hbm}}
         if router is not None and "value" in router:

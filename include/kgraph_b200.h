@@ -105,6 +105,34 @@ int kg_search_batch(kg_ctx *ctx, const float *queries, size_t nq, size_t q_strid
                     const kg_search_params *params, const uint32_t *K_per_q, const uint32_t *P_per_q,
                     size_t out_ld, uint32_t *ids, float *dists, uint32_t *counts, float *costs);
 
+/* Launch shape of the batched search kernel.  No counterpart in the reference
+ * (its search is one OpenMP thread per query, python-api.cpp:292-301): every
+ * shape walks exactly as the reference and returns the same bits; only the
+ * speed differs.
+ *   split            D-split: lanes of a warp per distance (2, 4 or 8); one
+ *                    warp evaluates 32/split candidates per pass
+ *   warps_per_block  query tile: queries (one warp each) per block, 1/2/4/8;
+ *                    0 = as many as fit 200 KB of shared memory, at most 8
+ *   prefetch         neighbour batches whose rows are prefetched into L2 ahead
+ *                    of the walk (0 or 2)
+ * ms / default_ms / variants are filled by kg_search_autotune. */
+typedef struct {
+    unsigned split, warps_per_block, prefetch;
+    float ms, default_ms;
+    unsigned variants;
+} kg_search_tuning;
+/* Times every shape on `queries` (a representative sample), checks that all
+ * of them return identical ids, distances, counts and costs, and keeps the
+ * fastest for the context's later searches.  With params->init > 0 the
+ * starting points are init_ids, nq rows of init_ld (else both are ignored).
+ * best may be NULL. */
+int kg_search_autotune(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes,
+                       const kg_search_params *params, const uint32_t *K_per_q, const uint32_t *P_per_q,
+                       const uint32_t *init_ids, size_t init_ld, kg_search_tuning *best);
+/* Sets / reads the context's search shape (split, warps_per_block, prefetch). */
+int kg_set_search_tuning(kg_ctx *ctx, const kg_search_tuning *t);
+int kg_get_search_tuning(kg_ctx *ctx, kg_search_tuning *t);
+
 /* KGraphImpl::reverse (kgraph.cpp:667-702) on the current graph. */
 int kg_reverse(kg_ctx *ctx, int rev_k);
 /* KGraph::prune (kgraph.h:180; kgraph.cpp:584-665) on the current graph. */

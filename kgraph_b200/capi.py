@@ -21,7 +21,8 @@ SYMBOLS = [
     "kg_graph_export", "kg_graph_import", "kg_search_batch", "kg_reverse", "kg_prune", "kg_last_timing",
     "kg_last_search_work", "kg_search_batch_noalloc", "kg_noalloc_scratch_bytes",
     "kg_router_params_default", "kg_router_train", "kg_router_seeds", "kg_router_gradients", "kg_last_router_timing",
-    "kg_set_join_precision", "kg_last_join_stats", "kg_last_build_graphs",
+    "kg_set_join_precision", "kg_last_join_stats", "kg_last_build_graphs", "kg_search_autotune",
+    "kg_set_search_tuning", "kg_get_search_tuning",
 ]
 
 JOIN = {"auto": 0, "fp32": 1, "bf16": 2, "bf16_always": 3}
@@ -54,6 +55,11 @@ class JoinStats(C.Structure):
                 ("mean_abs_err", C.c_double), ("max_rel_err", C.c_double), ("mean_rel_err", C.c_double),
                 ("max_err_over_margin", C.c_double), ("mean_err_over_margin", C.c_double),
                 ("tc_iterations", C.c_uint)]
+
+
+class SearchTuning(C.Structure):
+    _fields_ = [("split", C.c_uint), ("warps_per_block", C.c_uint), ("prefetch", C.c_uint), ("ms", C.c_float),
+                ("default_ms", C.c_float), ("variants", C.c_uint)]
 
 
 class SearchParams(C.Structure):
@@ -99,6 +105,10 @@ def lib():
         L.kg_set_join_precision.argtypes = [vp, C.c_int]
         L.kg_last_join_stats.argtypes = [vp, C.POINTER(JoinStats)]
         L.kg_last_build_graphs.argtypes = [vp, C.POINTER(C.c_uint)]
+        L.kg_search_autotune.argtypes = [vp, vp, sz, sz, C.POINTER(SearchParams), vp, vp, vp, sz,
+                                         C.POINTER(SearchTuning)]
+        L.kg_set_search_tuning.argtypes = [vp, C.POINTER(SearchTuning)]
+        L.kg_get_search_tuning.argtypes = [vp, C.POINTER(SearchTuning)]
         L.kg_index_params_default.argtypes = [C.POINTER(IndexParams)]
         L.kg_search_params_default.argtypes = [C.POINTER(SearchParams)]
         _lib = L
@@ -276,6 +286,28 @@ class Context:
         out = {f: getattr(st, f) for f, _ in JoinStats._fields_}
         out["mode"] = {1: "fp32", 2: "bf16"}.get(st.mode, "none")
         return out
+
+    def search_autotune(self, Q, K=10, P=100, M=0, S=10, T=1, epsilon=1e30, seed=1998, K_per_q=None, P_per_q=None,
+                        init=0, init_ids=None):
+        """Times every search shape on Q, checks they agree bit for bit, keeps the fastest."""
+        Q = np.ascontiguousarray(Q, np.float32)
+        p = SearchParams(K, M, P, S, T, epsilon, seed, init)
+        kq = None if K_per_q is None else np.ascontiguousarray(K_per_q, np.uint32)
+        pq = None if P_per_q is None else np.ascontiguousarray(P_per_q, np.uint32)
+        ii = None if init_ids is None else np.ascontiguousarray(init_ids, np.uint32)
+        t = SearchTuning()
+        self._check(self.L.kg_search_autotune(self.h, _ptr(Q), Q.shape[0], Q.strides[0], C.byref(p), _ptr(kq),
+                                              _ptr(pq), _ptr(ii), 0 if ii is None else ii.shape[1], C.byref(t)))
+        return {f: getattr(t, f) for f, _ in SearchTuning._fields_}
+
+    def set_search_tuning(self, split=4, warps_per_block=0, prefetch=2):
+        t = SearchTuning(split, warps_per_block, prefetch, 0.0, 0.0, 0)
+        self._check(self.L.kg_set_search_tuning(self.h, C.byref(t)))
+
+    def search_tuning(self):
+        t = SearchTuning()
+        self._check(self.L.kg_get_search_tuning(self.h, C.byref(t)))
+        return {"split": t.split, "warps_per_block": t.warps_per_block, "prefetch": t.prefetch}
 
     def build_graph_launches(self):
         """CUDA graph launches of the last build's iterations."""

@@ -113,6 +113,81 @@ __device__ __forceinline__ float group4_raw(const float *a, const float *b, int 
     return r;
 }
 
+// One canonical lane's step: acc += x*y (or (x-y)^2 for l2sqr), rounded product then rounded add.
+__device__ __forceinline__ void acc1(float &acc, float x, float y, int metric) {
+    if (metric == METRIC_L2SQR) { x = __fsub_rn(x, y); y = x; }
+    acc = __fadd_rn(acc, __fmul_rn(x, y));
+}
+
+// The canonical raw sum computed by a group of G consecutive lanes (the
+// "D-split"): lane t of the group owns canonical lanes (16/G)*t .. (16/G)*(t+1)-1,
+// so one warp evaluates 32/G distances per pass.  G = 4 is group4_raw.  The
+// lane sums are combined in exactly the canonical tree order, so every G gives
+// the same bits:
+//   G = 2  lane t holds lanes 8t..8t+7: a_j = x_j + x_{j+4} locally, the
+//          partner's a_j added (t_j), then (t_0 + t_1) + (t_2 + t_3);
+//   G = 8  lane t holds lanes 2t, 2t+1: + partner t^2 gives x_k + x_{k+4},
+//          + partner t^4 gives t_k, then t_{2t} + t_{2t+1} locally and the
+//          partner t^1 added.
+template <int G>
+__device__ __forceinline__ float groupG_raw(const float *a, const float *b, int d, int metric, int t, unsigned mask) {
+    static_assert(G == 2 || G == 4 || G == 8, "D-split of 2, 4 or 8 lanes");
+    if constexpr (G == 4) {
+        return group4_raw(a, b, d, metric, t, mask);
+    } else {
+        constexpr int W = 16 / G;
+        float acc[W];
+#pragma unroll
+        for (int j = 0; j < W; ++j) acc[j] = 0.f;
+        const int chunks = d >> 4;
+        for (int c = 0; c < chunks; ++c) {
+            const float *pa = a + 16 * c + W * t, *pb = b + 16 * c + W * t;
+            if constexpr (W == 8) {
+                const float4 x0 = ld4(pa), x1 = ld4(pa + 4), y0 = ld4(pb), y1 = ld4(pb + 4);
+                acc1(acc[0], x0.x, y0.x, metric); acc1(acc[1], x0.y, y0.y, metric);
+                acc1(acc[2], x0.z, y0.z, metric); acc1(acc[3], x0.w, y0.w, metric);
+                acc1(acc[4], x1.x, y1.x, metric); acc1(acc[5], x1.y, y1.y, metric);
+                acc1(acc[6], x1.z, y1.z, metric); acc1(acc[7], x1.w, y1.w, metric);
+            } else {
+                const float2 x = *reinterpret_cast<const float2 *>(pa), y = *reinterpret_cast<const float2 *>(pb);
+                acc1(acc[0], x.x, y.x, metric);
+                acc1(acc[1], x.y, y.y, metric);
+            }
+        }
+        float r;
+        if constexpr (W == 8) {
+            float tk[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const float aj = __fadd_rn(acc[j], acc[j + 4]);
+                tk[j] = __fadd_rn(aj, __shfl_xor_sync(mask, aj, 1));
+            }
+            r = __fadd_rn(__fadd_rn(tk[0], tk[1]), __fadd_rn(tk[2], tk[3]));
+        } else {
+            float u0 = __fadd_rn(acc[0], __shfl_xor_sync(mask, acc[0], 2));
+            float u1 = __fadd_rn(acc[1], __shfl_xor_sync(mask, acc[1], 2));
+            u0 = __fadd_rn(u0, __shfl_xor_sync(mask, u0, 4));
+            u1 = __fadd_rn(u1, __shfl_xor_sync(mask, u1, 4));
+            const float u = __fadd_rn(u0, u1);
+            r = __fadd_rn(u, __shfl_xor_sync(mask, u, 1));
+        }
+        int i = chunks << 4;
+        if (d - i >= 8) {   // as in group4_raw
+            for (int e = i + 8; i < e; ++i) {
+                float x = a[i], y = b[i];
+                if (metric == METRIC_L2SQR) { x = __fsub_rn(x, y); y = x; }
+                r = __fadd_rn(r, __fmul_rn(x, y));
+            }
+        }
+        for (; i < d; ++i) {
+            float x = a[i], y = b[i];
+            if (metric == METRIC_L2SQR) { x = __fsub_rn(x, y); y = x; }
+            r = __fmaf_rn(x, y, r);
+        }
+        return r;
+    }
+}
+
 __device__ __forceinline__ float finish_metric(float raw, float n1, float n2, int metric) {
     if (metric == METRIC_EUCLIDEAN) return __fsub_rn(__fadd_rn(n1, n2), raw);
     if (metric == METRIC_ANGULAR) return __fdiv_rn(-raw, __fmaf_rn(n1, n2, FLT_EPSILON));
@@ -138,6 +213,15 @@ __device__ __forceinline__ float pair_dist(const DataView &D, uint32_t i, uint32
 __device__ __forceinline__ float query_dist(const DataView &D, const float *q, float qn, uint32_t i, int t,
                                             unsigned mask) {
     float raw = group4_raw(D.X + (size_t)i * D.ld, q, D.d, D.metric, t, mask);
+    if (D.metric == METRIC_L2SQR) return raw;
+    return finish_metric(raw, D.norms[i], qn, D.metric);
+}
+
+// query_dist with a D-split of G lanes (groupG_raw); the same bits for every G.
+template <int G>
+__device__ __forceinline__ float query_dist_g(const DataView &D, const float *q, float qn, uint32_t i, int t,
+                                              unsigned mask) {
+    float raw = groupG_raw<G>(D.X + (size_t)i * D.ld, q, D.d, D.metric, t, mask);
     if (D.metric == METRIC_L2SQR) return raw;
     return finish_metric(raw, D.norms[i], qn, D.metric);
 }

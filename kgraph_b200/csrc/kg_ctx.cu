@@ -5,6 +5,7 @@
 #include <ctime>
 #include <map>
 #include <random>
+#include <limits>
 #include "kg_ctx.h"
 #include "kg_search.h"
 #include "kg_warp.cuh"
@@ -290,11 +291,14 @@ int ensure_search_layout(kg_ctx *ctx) {
 }
 }  // namespace kgb
 
-int kg_search_batch(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes,
-                    const kg_search_params *params, const uint32_t *K_per_q, const uint32_t *P_per_q,
-                    size_t out_ld, uint32_t *ids, float *dists, uint32_t *counts, float *costs) {
-    if (!ctx) return KG_E_INVALID;
-    Lock lk(ctx);
+}  // extern "C"
+
+namespace {
+
+// kg_search_batch with the context lock held, in launch shape `sh`.
+int search_locked(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes,
+                  const kg_search_params *params, const uint32_t *K_per_q, const uint32_t *P_per_q, size_t out_ld,
+                  uint32_t *ids, float *dists, uint32_t *counts, float *costs, const SearchShape &sh) {
     if (!ctx->has_data) return set_error(ctx, KG_E_RUNTIME, "no dataset");
     if (!params || !ids || !counts) return set_error(ctx, KG_E_INVALID, "bad arguments");
     if (nq == 0) return KG_OK;
@@ -451,7 +455,7 @@ int kg_search_batch(kg_ctx *ctx, const float *queries, size_t nq, size_t q_strid
 
     // visited sets: one per resident warp
     a.vwords = ((N + 31) / 32 + 3) / 4 * 4;
-    uint32_t slots = search_max_slots(a, ctx->num_sms);
+    uint32_t slots = search_max_slots(a, sh, ctx->num_sms);
     if ((e = ctx->visited.reserve((size_t)slots * a.vwords * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc visited");
     a.visited = ctx->visited.as<uint32_t>();
     a.visited_slots = slots;
@@ -461,7 +465,8 @@ int kg_search_batch(kg_ctx *ctx, const float *queries, size_t nq, size_t q_strid
     cudaMemsetAsync(ctx->counter.p, 0, 32, ctx->stream);
 
     cudaEventRecord(ctx->ev0, ctx->stream);
-    if ((e = launch_search(a, ctx->num_sms, ctx->stream, nullptr)) != cudaSuccess) return cuda_fail(ctx, e, "search launch");
+    if ((e = launch_search(a, sh, ctx->num_sms, ctx->stream, nullptr)) != cudaSuccess)
+        return cuda_fail(ctx, e, "search launch");
     cudaEventRecord(ctx->ev1, ctx->stream);
 
     if (!ids_dev) cudaMemcpyAsync(ids, a.out_ids, Q * out_ld * 4, cudaMemcpyDeviceToHost, ctx->stream);
@@ -472,6 +477,127 @@ int kg_search_batch(kg_ctx *ctx, const float *queries, size_t nq, size_t q_strid
     if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "search");
     cudaEventElapsedTime(&ctx->last_search_ms, ctx->ev0, ctx->ev1);
     return check_device_error(ctx, "search");
+}
+
+}  // namespace
+
+extern "C" {
+
+int kg_search_batch(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes,
+                    const kg_search_params *params, const uint32_t *K_per_q, const uint32_t *P_per_q,
+                    size_t out_ld, uint32_t *ids, float *dists, uint32_t *counts, float *costs) {
+    if (!ctx) return KG_E_INVALID;
+    Lock lk(ctx);
+    return search_locked(ctx, queries, nq, q_stride_bytes, params, K_per_q, P_per_q, out_ld, ids, dists, counts,
+                         costs, ctx->search_shape);
+}
+
+namespace {
+SearchShape shape_of(const kg_search_tuning &t) {
+    SearchShape sh;
+    sh.split = t.split;
+    sh.warps_per_block = t.warps_per_block;
+    sh.prefetch = t.prefetch;
+    return sh;
+}
+}  // namespace
+
+int kg_set_search_tuning(kg_ctx *ctx, const kg_search_tuning *t) {
+    if (!ctx || !t) return KG_E_INVALID;
+    Lock lk(ctx);
+    const SearchShape sh = shape_of(*t);
+    if (!search_shape_valid(sh) || sh.split == 0)
+        return set_error(ctx, KG_E_INVALID, "search tuning: split must be 2, 4 or 8, warps_per_block 0, 1, 2, 4 or "
+                                            "8, prefetch 0 or 2");
+    ctx->search_shape = sh;
+    return KG_OK;
+}
+
+int kg_get_search_tuning(kg_ctx *ctx, kg_search_tuning *t) {
+    if (!ctx || !t) return KG_E_INVALID;
+    Lock lk(ctx);
+    *t = kg_search_tuning{};
+    t->split = ctx->search_shape.split;
+    t->warps_per_block = ctx->search_shape.warps_per_block;
+    t->prefetch = ctx->search_shape.prefetch;
+    return KG_OK;
+}
+
+int kg_search_autotune(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes,
+                       const kg_search_params *params, const uint32_t *K_per_q, const uint32_t *P_per_q,
+                       const uint32_t *init_ids, size_t init_ld, kg_search_tuning *best) {
+    if (!ctx) return KG_E_INVALID;
+    Lock lk(ctx);
+    if (!params || !queries || nq == 0) return set_error(ctx, KG_E_INVALID, "bad arguments");
+    // outputs on the host, one row of Kmax per query; every shape must give the same bits
+    uint32_t Kmax = params->K;
+    if (K_per_q) {
+        std::vector<uint32_t> hK(nq);
+        cudaMemcpy(hK.data(), K_per_q, nq * sizeof(uint32_t), cudaMemcpyDefault);
+        Kmax = *std::max_element(hK.begin(), hK.end());
+    }
+    const size_t ld = std::max<uint32_t>(Kmax, std::max<uint32_t>(params->init, 1u));
+    std::vector<uint32_t> ids(nq * ld), ref_ids, init_rows;
+    std::vector<float> dists(nq * ld), costs(nq), ref_d, ref_c;
+    std::vector<uint32_t> counts(nq), ref_n;
+    if (params->init) {   // starting points are an input of every run: keep a copy
+        if (!init_ids || init_ld < params->init)
+            return set_error(ctx, KG_E_INVALID, "kg_search_autotune: init > 0 needs init_ids rows of init_ld >= init");
+        std::vector<uint32_t> rows(nq * init_ld);
+        cudaMemcpy(rows.data(), init_ids, rows.size() * 4, cudaMemcpyDefault);
+        init_rows.assign(nq * ld, 0u);
+        for (size_t q = 0; q < nq; ++q)
+            std::copy(rows.begin() + q * init_ld, rows.begin() + q * init_ld + params->init, init_rows.begin() + q * ld);
+    }
+    const SearchShape def = ctx->search_shape;
+    SearchShape top = def;
+    float top_ms = std::numeric_limits<float>::max(), def_ms = 0.f;
+    unsigned variants = 0;
+    auto run = [&](const SearchShape &sh, float *ms) -> int {
+        float bestv = std::numeric_limits<float>::max();
+        for (int rep = 0; rep < 3; ++rep) {   // one warm-up, the faster of two timed runs
+            if (params->init) ids = init_rows;
+            int r = search_locked(ctx, queries, nq, q_stride_bytes, params, K_per_q, P_per_q, ld, ids.data(),
+                                  dists.data(), counts.data(), costs.data(), sh);
+            if (r != KG_OK) return r;
+            if (rep > 0) bestv = std::min(bestv, ctx->last_search_ms);
+        }
+        *ms = bestv;
+        return KG_OK;
+    };
+    // the default shape first: its results are the ones every other shape must reproduce
+    int r = run(def, &def_ms);
+    if (r != KG_OK) return r;
+    ref_ids = ids; ref_d = dists; ref_n = counts; ref_c = costs;
+    top_ms = def_ms;
+    ++variants;
+    for (uint32_t split : {2u, 4u, 8u})
+        for (uint32_t wpb : {2u, 4u, 8u})
+            for (uint32_t pf : {0u, 2u}) {
+                SearchShape sh;
+                sh.split = split; sh.warps_per_block = wpb; sh.prefetch = pf;
+                float ms = 0.f;
+                if ((r = run(sh, &ms)) != KG_OK) return r;
+                ++variants;
+                if (std::memcmp(ids.data(), ref_ids.data(), ids.size() * 4) ||
+                    std::memcmp(dists.data(), ref_d.data(), dists.size() * 4) ||
+                    std::memcmp(counts.data(), ref_n.data(), counts.size() * 4) ||
+                    std::memcmp(costs.data(), ref_c.data(), costs.size() * 4))
+                    return set_error(ctx, KG_E_RUNTIME, "kg_search_autotune: search shapes disagree (split " +
+                                                            std::to_string(split) + ")");
+                if (ms < top_ms) { top_ms = ms; top = sh; }
+            }
+    ctx->search_shape = top;
+    if (best) {
+        *best = kg_search_tuning{};
+        best->split = top.split;
+        best->warps_per_block = top.warps_per_block;
+        best->prefetch = top.prefetch;
+        best->ms = top_ms;
+        best->default_ms = def_ms;
+        best->variants = variants;
+    }
+    return KG_OK;
 }
 
 }  // extern "C"

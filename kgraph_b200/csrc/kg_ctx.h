@@ -6,6 +6,7 @@
 #include <vector>
 #include <cuda_runtime.h>
 #include "kg_common.cuh"
+#include "kg_search.h"
 #include "../../include/kgraph_b200.h"
 
 namespace kgb {
@@ -66,6 +67,7 @@ struct kg_ctx {
     // search-side copy of the graph: ELL rows of the first ell_w neighbours + {M, degree}
     kgb::DevBuf ell, meta;
     uint32_t ell_w = 0;
+    kgb::SearchShape search_shape;   // launch shape of the search kernel (kg_search_autotune)
     uint64_t layout_version = ~0ull;
 
     // scratch

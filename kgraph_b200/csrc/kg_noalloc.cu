@@ -139,7 +139,7 @@ extern "C" int kg_search_batch_noalloc(kg_ctx *ctx, const float *queries, size_t
     a.vwords = ((N + 31) / 32 + 3) / 4 * 4;
     const size_t per_slot = (size_t)a.vwords * 4;
     const size_t fit = (SCRATCH_BYTES - off) / per_slot;
-    const uint32_t per_sm_slots = search_max_slots(a, 1);
+    const uint32_t per_sm_slots = search_max_slots(a, ctx->search_shape, 1);
     if (fit < per_sm_slots)
         return set_error(ctx, KG_E_INVALID, "kg_search_batch_noalloc: N = " + std::to_string(N) +
                                                  " needs more visited-set scratch than the " +
@@ -166,7 +166,7 @@ extern "C" int kg_search_batch_noalloc(kg_ctx *ctx, const float *queries, size_t
     cudaMemsetAsync(base, 0, HEADER_BYTES, st);        // counter, error word, work counters start at zero
     cudaMemsetAsync(seed_index, 0, nq * 4, st);         // one P for the batch: every query uses list 0
     cudaEventRecord(ctx->ev0, st);
-    if ((e = launch_search(a, sms, st, nullptr)) != cudaSuccess) return cuda_fail(ctx, e, "noalloc search launch");
+    if ((e = launch_search(a, ctx->search_shape, sms, st, nullptr)) != cudaSuccess) return cuda_fail(ctx, e, "noalloc search launch");
     cudaEventRecord(ctx->ev1, st);
     uint32_t err = 0;
     cudaMemcpyAsync(&err, a.err, 4, cudaMemcpyDeviceToHost, st);

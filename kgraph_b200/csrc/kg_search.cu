@@ -17,6 +17,7 @@
 // pure), then inserted one by one in order, which is what the reference's
 // interleaved loop produces.  With the canonical distance this reproduces
 // the reference's ids, distances, result count and SearchInfo.cost exactly.
+#include <algorithm>
 #include "kg_common.cuh"
 #include "kg_warp.cuh"
 #include "kg_sort.h"
@@ -87,14 +88,16 @@ __device__ __forceinline__ uint32_t neighbour(const SearchArgs &a, uint32_t node
     return a.nbr[a.offsets[node] + p];
 }
 
-// Distances for cnt candidates cid[0..cnt) -> cd[], 8 per pass (4-lane groups).
+// Distances for cnt candidates cid[0..cnt) -> cd[], 32/G per pass (G-lane groups).
+template <int G>
 __device__ __forceinline__ void batch_dist(const SearchArgs &a, const WarpSmem &s, float qn, uint32_t cnt,
                                            int lane) {
-    const int g = lane >> 2, t = lane & 3;
-    for (uint32_t base = 0; base < cnt; base += 8) {
+    constexpr uint32_t PER = 32 / G;
+    const int g = lane / G, t = lane % G;
+    for (uint32_t base = 0; base < cnt; base += PER) {
         uint32_t c = base + g;
         uint32_t id = c < cnt ? s.cid[c] : 0u;
-        float dd = query_dist(a.D, s.q, qn, id, t, FULL);
+        float dd = query_dist_g<G>(a.D, s.q, qn, id, t, FULL);
         if (c < cnt && t == 0) s.cd[c] = dd;
     }
     __syncwarp();
@@ -102,6 +105,7 @@ __device__ __forceinline__ void batch_dist(const SearchArgs &a, const WarpSmem &
 
 // SearchOracle::search (kgraph.cpp:231-252) by one warp: every row in id
 // order, epsilon filter, sorted insert into K slots (+1 overflow).
+template <int G>
 __device__ uint32_t warp_bruteforce(const SearchArgs &a, const WarpSmem &s, float qn, uint32_t K, int lane) {
     const uint32_t N = a.D.n;
     uint32_t L = 0;
@@ -109,7 +113,7 @@ __device__ uint32_t warp_bruteforce(const SearchArgs &a, const WarpSmem &s, floa
         uint32_t cnt = min(32u, N - base);
         if (lane < (int)cnt) s.cid[lane] = base + lane;
         __syncwarp();
-        batch_dist(a, s, qn, cnt, lane);
+        batch_dist<G>(a, s, qn, cnt, lane);
         for (uint32_t c = 0; c < cnt; ++c) {
             float dd = s.cd[c];
             if (dd > a.epsilon) continue;
@@ -122,23 +126,25 @@ __device__ uint32_t warp_bruteforce(const SearchArgs &a, const WarpSmem &s, floa
     return L;
 }
 
-// Distances of the candidate lanes in `cm` (each holds its id), computed 8 at a
-// time by the 4-lane groups; every candidate lane returns its own distance.
+// Distances of the candidate lanes in `cm` (each holds its id), computed 32/G
+// at a time by the G-lane groups; every candidate lane returns its own distance.
 // Everything stays in registers (no shared-memory staging, so no barrier waits
 // on memory operations still in flight).
+template <int G>
 __device__ __forceinline__ float warp_cand_dist(const SearchArgs &a, const float *q, float qn, unsigned cm, bool cand,
                                                uint32_t id, int lane) {
-    const int g = lane >> 2, t = lane & 3;
+    constexpr uint32_t PER = 32 / G;
+    const int g = lane / G, t = lane % G;
     const uint32_t n = __popc(cm);
     const uint32_t my = __popc(cm & ((1u << lane) - 1u));
     float mine = 0.f;
-    for (uint32_t base = 0; base < n; base += 8) {
+    for (uint32_t base = 0; base < n; base += PER) {
         const uint32_t i = base + g;
         const int src = i < n ? (int)__fns(cm, 0, i + 1) : 0;
         const uint32_t cid = __shfl_sync(FULL, id, src);
-        const float dd = query_dist(a.D, q, qn, i < n ? cid : 0u, t, FULL);
-        const float got = __shfl_sync(FULL, dd, (int)(4 * (my & 7)));
-        if (cand && (my >> 3) == (base >> 3)) mine = got;
+        const float dd = query_dist_g<G>(a.D, q, qn, i < n ? cid : 0u, t, FULL);
+        const float got = __shfl_sync(FULL, dd, (int)(G * (my % PER)));
+        if (cand && my / PER == base / PER) mine = got;
     }
     return mine;
 }
@@ -158,6 +164,9 @@ __device__ __forceinline__ bool visited_test_set(uint32_t *vis, uint32_t id) {
 
 }  // namespace
 
+// G: lanes per distance (the D-split, 32/G candidates per pass); PF: neighbour
+// batches whose rows are prefetched into L2 ahead of the walk.
+template <int G, int PF>
 __global__ void __launch_bounds__(256, 4) search_kernel(SearchArgs a) {
     extern __shared__ __align__(16) char smem[];
     const int lane = threadIdx.x & 31;
@@ -195,7 +204,7 @@ __global__ void __launch_bounds__(256, 4) search_kernel(SearchArgs a) {
         float *out_d = a.out_dists ? a.out_dists + (size_t)qi * a.out_ld : nullptr;
 
         if (P >= N) {   // kgraph.cpp:427-433: brute force, cost 1
-            count = warp_bruteforce(a, s, qn, K, lane);
+            count = warp_bruteforce<G>(a, s, qn, K, lane);
             for (uint32_t k = lane; k < count; k += 32) {
                 out_i[k] = s.pid[k] & ID_MASK;
                 if (out_d) out_d[k] = s.pd[k];
@@ -253,7 +262,7 @@ __global__ void __launch_bounds__(256, 4) search_kernel(SearchArgs a) {
                 uint32_t cnt = min(32u, L - base);
                 if (j < L) s.cid[lane] = bad ? 0u : id;
                 __syncwarp();
-                batch_dist(a, s, qn, cnt, lane);
+                batch_dist<G>(a, s, qn, cnt, lane);
                 if (j < L) { s.pd[j] = s.cd[lane]; s.pid[j] = id | FLAG_BIT; }
                 __syncwarp();
             }
@@ -341,13 +350,15 @@ __global__ void __launch_bounds__(256, 4) search_kernel(SearchArgs a) {
                             if ((uint32_t)cc == c) { id = wid[cc]; uv = wuv[cc]; }
                         const bool cand = uv && (uint32_t)lane >= lo && (uint32_t)lane < hi;
                         const unsigned cm = __ballot_sync(FULL, cand);
-                        // L2 prefetch of the rows the next two batches of this entry will
+                        // L2 prefetch of the rows the next PF batches of this entry will
                         // read (unvisited window ids), behind this batch's loads
+                        if constexpr (PF > 0) {
 #pragma unroll
-                        for (int cc = 0; cc < 4; ++cc) {
-                            const uint32_t pos = wlo + 32 * cc + lane;
-                            if (wuv[cc] && pos >= p1 && pos < p1 + 2 * S && pos < whi)
-                                prefetch_row(a.D, wid[cc]);
+                            for (int cc = 0; cc < 4; ++cc) {
+                                const uint32_t pos = wlo + 32 * cc + lane;
+                                if (wuv[cc] && pos >= p1 && pos < p1 + PF * S && pos < whi)
+                                    prefetch_row(a.D, wid[cc]);
+                            }
                         }
                         if (cm) {
                             // All three in flight together: the exact test-and-set of the
@@ -359,7 +370,7 @@ __global__ void __launch_bounds__(256, 4) search_kernel(SearchArgs a) {
                                 isnew = !(atomicOr(vis + (id >> 5), bit) & bit);
                                 aM = actual_M(a, a.Mp, id);
                             }
-                            const float dd = warp_cand_dist(a, s.q, qn, cm, cand, id, lane);
+                            const float dd = warp_cand_dist<G>(a, s.q, qn, cm, cand, id, lane);
                             const unsigned nm = __ballot_sync(FULL, isnew);
                             n_comps += __popc(nm);
                             // A full pool takes a candidate only below its last entry: one at or
@@ -425,18 +436,48 @@ size_t search_warp_smem_bytes(uint32_t ld, uint32_t cap, uint32_t rcap) {
     return (b + 15) & ~size_t(15);
 }
 
-cudaError_t launch_search(SearchArgs &a, int num_sms, cudaStream_t st, uint32_t *grid_out) {
+namespace {
+
+using SearchFn = void (*)(SearchArgs);
+// The compiled (D-split, prefetch) variants.
+SearchFn search_fn(uint32_t split, uint32_t prefetch) {
+    const bool pf = prefetch > 0;
+    switch (split) {
+        case 2: return pf ? search_kernel<2, 2> : search_kernel<2, 0>;
+        case 8: return pf ? search_kernel<8, 2> : search_kernel<8, 0>;
+        default: return pf ? search_kernel<4, 2> : search_kernel<4, 0>;
+    }
+}
+
+// Warps per block: the requested query tile, or as many as fit 200 KB of
+// shared memory (at most 8); halved until the block fits.
+uint32_t pick_wpb(const SearchShape &sh, size_t warp_bytes) {
+    uint32_t wpb = sh.warps_per_block ? std::min<uint32_t>(sh.warps_per_block, 8) : 8;
+    while (wpb > 1 && (size_t)wpb * warp_bytes > 200 * 1024) wpb >>= 1;
+    return wpb;
+}
+
+}  // namespace
+
+bool search_shape_valid(const SearchShape &sh) {
+    const bool split_ok = sh.split == 0 || sh.split == 2 || sh.split == 4 || sh.split == 8;
+    const bool wpb_ok = sh.warps_per_block == 0 || sh.warps_per_block == 1 || sh.warps_per_block == 2 ||
+                        sh.warps_per_block == 4 || sh.warps_per_block == 8;
+    const bool pf_ok = sh.prefetch == 0 || sh.prefetch == 2;
+    return split_ok && wpb_ok && pf_ok;
+}
+
+cudaError_t launch_search(SearchArgs &a, const SearchShape &sh, int num_sms, cudaStream_t st, uint32_t *grid_out) {
     a.warp_smem_bytes = (uint32_t)search_warp_smem_bytes(a.D.ld, a.cap, a.rcap);
-    // Warps per block: as many as fit 200 KB of shared memory, at most 8.
-    uint32_t wpb = 8;
-    while (wpb > 1 && (size_t)wpb * a.warp_smem_bytes > 200 * 1024) wpb >>= 1;
+    const uint32_t wpb = pick_wpb(sh, a.warp_smem_bytes);
     if ((size_t)wpb * a.warp_smem_bytes > 227 * 1024) return cudaErrorInvalidValue;
     a.warps_per_block = wpb;
     size_t smem = (size_t)wpb * a.warp_smem_bytes;
-    cudaError_t e = cudaFuncSetAttribute(search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    SearchFn fn = search_fn(sh.split, sh.prefetch);
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_kernel, wpb * 32, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, wpb * 32, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     uint32_t grid = (uint32_t)(num_sms * per_sm);
@@ -445,18 +486,18 @@ cudaError_t launch_search(SearchArgs &a, int num_sms, cudaStream_t st, uint32_t 
     if (grid < 1) grid = 1;
     if (grid_out) *grid_out = grid;
     if (grid * wpb > a.visited_slots) return cudaErrorInvalidValue;
-    search_kernel<<<grid, wpb * 32, smem, st>>>(a);
+    fn<<<grid, wpb * 32, smem, st>>>(a);
     return cudaGetLastError();
 }
 
-uint32_t search_max_slots(const SearchArgs &a, int num_sms) {
-    size_t wb = search_warp_smem_bytes(a.D.ld, a.cap, a.rcap);
-    uint32_t wpb = 8;
-    while (wpb > 1 && (size_t)wpb * wb > 200 * 1024) wpb >>= 1;
-    size_t smem = (size_t)wpb * wb;
-    cudaFuncSetAttribute(search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+uint32_t search_max_slots(const SearchArgs &a, const SearchShape &sh, int num_sms) {
+    const size_t wb = search_warp_smem_bytes(a.D.ld, a.cap, a.rcap);
+    const uint32_t wpb = pick_wpb(sh, wb);
+    const size_t smem = (size_t)wpb * wb;
+    SearchFn fn = search_fn(sh.split, sh.prefetch);
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_kernel, wpb * 32, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, wpb * 32, smem);
     if (per_sm < 1) per_sm = 1;
     return (uint32_t)(num_sms * per_sm) * wpb;
 }

@@ -36,9 +36,18 @@ struct SearchArgs {
     uint32_t warps_per_block, warp_smem_bytes;   // filled by launch_search
 };
 
+// Launch shape of the search kernel: the D-split (lanes per distance, 2/4/8;
+// 32/split candidates per pass), the query tile (warps = queries per block,
+// 1/2/4/8; 0 = as many as fit, at most 8) and the L2 prefetch depth (0 or 2
+// neighbour batches).  Every shape computes the same bits.
+struct SearchShape {
+    uint32_t split = 4, warps_per_block = 0, prefetch = 2;
+};
+bool search_shape_valid(const SearchShape &sh);
+
 size_t search_warp_smem_bytes(uint32_t ld, uint32_t cap, uint32_t rcap);
 // Upper bound of concurrently resident warps (= visited slots needed).
-uint32_t search_max_slots(const SearchArgs &a, int num_sms);
-cudaError_t launch_search(SearchArgs &a, int num_sms, cudaStream_t st, uint32_t *grid_out);
+uint32_t search_max_slots(const SearchArgs &a, const SearchShape &sh, int num_sms);
+cudaError_t launch_search(SearchArgs &a, const SearchShape &sh, int num_sms, cudaStream_t st, uint32_t *grid_out);
 
 }  // namespace kgb
