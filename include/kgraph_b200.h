@@ -165,25 +165,36 @@ size_t kg_noalloc_scratch_bytes(void);
  * seeds in ids, doc/params.md "User-Provided Starting Points").  Training
  * (on the GPU): k-means of the dataset into `clusters` entry clusters (entry
  * node = the member nearest the centroid); labels = the cluster of the best
- * node the plain search (P = label_P) finds for each training query; MLP
+ * node the plain search (P = label_P) finds for each training query (then
+ * refined, see `refine`); MLP
  * d -> hidden -> hidden -> clusters (ReLU), BF16 weights with FP32 masters and
  * accumulation, softmax cross-entropy, Adam. */
 typedef struct {
     unsigned clusters, hidden, kmeans_iters, label_P, epochs, batch;
     float lr;
     unsigned seed;
+    unsigned entries;   /* fine clusters (entry nodes) per cluster, 1..16 */
+    unsigned probe;     /* clusters whose entry nodes are ranked per query, 1..32 */
+    unsigned refine;    /* refinement rounds (0..8): each relabels a training query with the node the
+                           router-seeded walk (P = refine_P) finds when it is closer than its label,
+                           then trains `epochs` more */
+    unsigned refine_P;
 } kg_router_params;
 typedef struct {
     unsigned steps;
     float final_loss, train_accuracy;
-    unsigned empty_clusters;
+    unsigned empty_clusters;     /* clusters without an entry node */
+    unsigned entries;            /* entry nodes over all clusters */
+    unsigned component_entries;  /* of which added for graph components no fine cluster reached */
+    unsigned relabelled;         /* training labels changed by the refinement */
 } kg_router_info;
 void kg_router_params_default(kg_router_params *p);
 /* Trains the router on the context's dataset and graph. */
 int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const float *train_queries, size_t ntrain,
                     size_t q_stride_bytes, kg_router_info *info);
-/* Entry nodes of the m most likely clusters of each query (best first), rows of
- * out_ld; pass them to kg_search_batch as ids with params->init = m (m < K). */
+/* Seeds of each query: the entry nodes of its `probe` most likely clusters,
+ * ranked by exact FP32 distance to the query, the m nearest first (rows of
+ * out_ld); pass them to kg_search_batch as ids with params->init = m (m < K). */
 int kg_router_seeds(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes, unsigned m, uint32_t *seeds,
                     size_t out_ld);
 /* Mean loss and gradients (W1|b1|W2|b2|W3|b3, FP32, row-major in x out) of the

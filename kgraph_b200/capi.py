@@ -41,12 +41,14 @@ class IndexInfo(C.Structure):
 
 class RouterParams(C.Structure):
     _fields_ = [("clusters", C.c_uint), ("hidden", C.c_uint), ("kmeans_iters", C.c_uint), ("label_P", C.c_uint),
-                ("epochs", C.c_uint), ("batch", C.c_uint), ("lr", C.c_float), ("seed", C.c_uint)]
+                ("epochs", C.c_uint), ("batch", C.c_uint), ("lr", C.c_float), ("seed", C.c_uint),
+                ("entries", C.c_uint), ("probe", C.c_uint), ("refine", C.c_uint), ("refine_P", C.c_uint)]
 
 
 class RouterInfo(C.Structure):
     _fields_ = [("steps", C.c_uint), ("final_loss", C.c_float), ("train_accuracy", C.c_float),
-                ("empty_clusters", C.c_uint)]
+                ("empty_clusters", C.c_uint), ("entries", C.c_uint), ("component_entries", C.c_uint),
+                ("relabelled", C.c_uint)]
 
 
 class JoinStats(C.Structure):

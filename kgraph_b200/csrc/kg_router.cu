@@ -11,20 +11,29 @@
 // P ~ 50..100.
 //
 // What runs on the GPU, all in this file:
-//   * entry clusters: k-means (C clusters) of the dataset -- assignment by a
-//     BF16 x BF16 -> FP32 tiled GEMM against the centroids plus an argmin, update
-//     by atomics; per cluster the member nearest its centroid is the entry node;
+//   * entry clusters, two levels: k-means of the dataset into C x E fine
+//     clusters (assignment by a BF16 x BF16 -> FP32 tiled GEMM against the
+//     centroids plus an argmin, update by atomics), the member nearest each fine
+//     centroid being a fine entry node; then k-means of the fine centroids into
+//     the C clusters the MLP predicts, each owning the entry nodes of its fine
+//     clusters;
 //   * the MLP  D -> H -> H -> C  (ReLU), BF16 weights with FP32 master copies,
 //     FP32 accumulation: forward, softmax cross-entropy, backward and Adam, every
 //     step by the kernels below;
 //   * training pairs: (query, cluster of the best node the plain search finds);
-//   * inference: top-m clusters per query -> their entry nodes.
+//   * inference: the `probe` most likely clusters per query, their fine entry
+//     nodes ranked by exact FP32 distance to the query, the m nearest are the
+//     seeds.  The second level lets C logits address more regions than C: a
+//     mixture with more components than clusters still gets a seed in the
+//     query's own component.
 #include <cuda_bf16.h>
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <random>
 #include <vector>
 #include "kg_ctx.h"
+#include "kg_warp.cuh"
 
 namespace kgb {
 
@@ -260,7 +269,82 @@ __global__ void topm_kernel(const float *Z, int rows, int C, int m, const uint32
         }
         if (bi < 0) bi = 0;
         if ((bi & 31) == lane) { const int s = bi >> 5; taken[s >> 6] |= 1ull << (s & 63); }
-        if (lane == 0) out[(size_t)r * out_ld + t] = entry[bi];
+        if (lane == 0) out[(size_t)r * out_ld + t] = entry ? entry[bi] : (uint32_t)bi;
+    }
+}
+
+// FP32 centroids from rows of the BF16 feature matrix.
+__global__ void init_centroids_kernel(const __nv_bfloat16 *F, uint32_t D, const uint32_t *rows, uint32_t C,
+                                      float *cent) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (size_t)C * D;
+         i += (size_t)gridDim.x * blockDim.x)
+        cent[i] = __bfloat162float(F[(size_t)rows[i / D] * D + i % D]);
+}
+
+constexpr int RANK_CAND = 256;   // fine entry nodes ranked per query, at most
+constexpr int RANK_WARPS = 8;
+
+// Seeds of one query per warp: the fine entry nodes of its `probe` most likely
+// clusters (topc), their canonical FP32 distances to the query, and the m
+// nearest (ties: earlier candidate first).  Fewer than m candidates repeat the
+// nearest one.  Q holds the queries' FP32 rows of D.d floats.
+__global__ void __launch_bounds__(RANK_WARPS * 32) seed_rank_kernel(DataView D, const float *Q, int rows,
+                                                                   const uint32_t *topc, int probe,
+                                                                   const uint32_t *eoff, const uint32_t *eids, int m,
+                                                                   uint32_t *out, int out_ld) {
+    extern __shared__ __align__(16) float rank_smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    float *q = rank_smem + (size_t)w * (D.ld + 2 * RANK_CAND);
+    uint32_t *cid = reinterpret_cast<uint32_t *>(q + D.ld);
+    float *cd = q + D.ld + RANK_CAND;
+    for (int r = blockIdx.x * RANK_WARPS + w; r < rows; r += gridDim.x * RANK_WARPS) {
+        for (uint32_t j = lane; j < D.ld; j += 32) q[j] = j < D.d ? Q[(size_t)r * D.d + j] : 0.f;
+        // candidate ids, in cluster-rank order
+        int n = 0;
+        for (int t = 0; t < probe; ++t) {
+            const uint32_t c = topc[(size_t)r * probe + t];
+            const uint32_t a = eoff[c], b = eoff[c + 1];
+            for (uint32_t k = a + lane; k < b; k += 32) {
+                const int at = n + (int)(k - a);
+                if (at < RANK_CAND) cid[at] = eids[k];
+            }
+            n = min(RANK_CAND, n + (int)(b - a));
+        }
+        __syncwarp();
+        float qn = 0.f;
+        if (D.metric != METRIC_L2SQR) qn = norm_term(group4_raw(q, q, D.d, METRIC_EUCLIDEAN, lane & 3, FULL), D.metric);
+        const int g = lane >> 2, t = lane & 3;
+        for (int base = 0; base < n; base += 8) {
+            const int i = base + g;
+            const float dd = query_dist(D, q, qn, i < n ? cid[i] : 0u, t, FULL);
+            if (i < n && t == 0) cd[i] = dd;
+        }
+        __syncwarp();
+        // m rounds of a warp argmin over the remaining candidates
+        uint32_t taken = 0;   // bit s: this lane's candidate lane + 32 s is taken
+        uint32_t first = 0;
+        for (int k = 0; k < m; ++k) {
+            float bv = INFINITY;
+            int bi = -1;
+            for (int i = lane, sl = 0; i < n; i += 32, ++sl) {
+                if ((taken >> sl) & 1u) continue;
+                if (cd[i] < bv) { bv = cd[i]; bi = i; }
+            }
+            for (int o = 16; o; o >>= 1) {
+                const float ov = __shfl_xor_sync(FULL, bv, o);
+                const int oi = __shfl_xor_sync(FULL, bi, o);
+                if (oi >= 0 && (bi < 0 || ov < bv || (ov == bv && oi < bi))) { bv = ov; bi = oi; }
+            }
+            uint32_t pick;
+            if (bi < 0) pick = first;   // candidates exhausted
+            else {
+                pick = cid[bi];
+                if ((bi & 31) == lane) taken |= 1u << (bi >> 5);
+            }
+            if (k == 0) first = pick;
+            if (lane == 0) out[(size_t)r * out_ld + k] = pick;
+        }
+        __syncwarp();
     }
 }
 
@@ -277,13 +361,16 @@ int blocks_for(size_t n, int per = 256) { return (int)std::min<size_t>((n + per 
 // ---------------------------------------------------------------------------
 // Router state (device): weights, Adam moments, activations for one batch.
 struct RouterState {
-    uint32_t D = 0, H = 0, C = 0, batch = 0;
+    uint32_t D = 0, H = 0, C = 0, batch = 0, probe = 1;
+    uint32_t entries_total = 0, component_entries = 0;   // entry nodes; of which added for uncovered components
     bool trained = false;
-    DevBuf mean, inv_std, entry;                 // normalisation, entry node per cluster
+    DevBuf mean, inv_std;                        // normalisation
+    DevBuf eoff, eids;                           // per cluster: its fine entry nodes (CSR)
     DevBuf w[3], b[3], wb[3], gw[3], gb[3], mw[3], vw[3], mb[3], vb[3];
-    DevBuf X, H1, H1b, H2, H2b, Z, dZ, dZb, dH, dHb, lab, scal;
+    DevBuf X, H1, H1b, H2, H2b, Z, dZ, dZb, dH, dHb, lab, scal, topc;
     void release() {
-        DevBuf *all[] = {&mean, &inv_std, &entry, &X, &H1, &H1b, &H2, &H2b, &Z, &dZ, &dZb, &dH, &dHb, &lab, &scal};
+        DevBuf *all[] = {&mean, &inv_std, &eoff, &eids, &X, &H1, &H1b, &H2, &H2b, &Z, &dZ, &dZb, &dH, &dHb, &lab,
+                         &scal, &topc};
         for (DevBuf *p : all) p->release();
         for (int l = 0; l < 3; ++l) {
             DevBuf *ps[] = {&w[l], &b[l], &wb[l], &gw[l], &gb[l], &mw[l], &vw[l], &mb[l], &vb[l]};
@@ -362,6 +449,108 @@ void backward(cudaStream_t st, RouterState &r, int B) {
     colsum_kernel<<<(r.H + 255) / 256, 256, 0, st>>>(r.dZ.as<float>(), B, r.H, r.gb[0].as<float>());
 }
 
+// Weakly connected components of the CSR graph by minimum-label propagation:
+// every edge pulls both endpoints' labels down to the smaller one, then labels
+// jump to their label's label; repeated until nothing changes.  The label of a
+// component is its smallest node id.
+__global__ void cc_hook_kernel(uint32_t N, const uint64_t *off, const uint32_t *nbr, uint32_t *lab, uint32_t *changed) {
+    const int lane = threadIdx.x & 31;
+    for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < N; u += (gridDim.x * blockDim.x) >> 5) {
+        const uint64_t a = off[u], b = off[u + 1];
+        bool ch = false;
+        for (uint64_t k = a + lane; k < b; k += 32) {
+            const uint32_t v = nbr[k];
+            if (v >= N) continue;
+            const uint32_t lu = lab[u], lv = lab[v];
+            if (lu < lv) ch |= atomicMin(lab + v, lu) > lu;
+            else if (lv < lu) ch |= atomicMin(lab + u, lv) > lv;
+        }
+        if (__any_sync(0xFFFFFFFFu, ch) && lane == 0) *changed = 1u;
+    }
+}
+
+__global__ void cc_jump_kernel(uint32_t N, uint32_t *lab) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < N; v += gridDim.x * blockDim.x) {
+        uint32_t l = lab[v];
+        while (lab[l] < l) l = lab[l];   // labels only point down, so this ends
+        lab[v] = l;
+    }
+}
+
+__global__ void iota_kernel(uint32_t N, uint32_t *lab) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < N; v += gridDim.x * blockDim.x) lab[v] = v;
+}
+
+// Scratch of one k-means run, released on scope exit.
+struct KMeansBufs {
+    DevBuf work, rows;
+    ~KMeansBufs() { work.release(); rows.release(); }
+};
+
+// Lloyd's k-means of n BF16 rows F (n x D) into C centroids started at the rows
+// `seed_rows`: `iters` updates, then a final assignment into lab[n] / best[n]
+// (|c|^2 - 2 f.c of the chosen centroid).  The BF16 centroids end in
+// *centb_out (inside kb.work); `block` holds one block of F.C^T.
+cudaError_t kmeans_run(cudaStream_t st, const __nv_bfloat16 *F, uint32_t n, uint32_t D, uint32_t C, uint32_t iters,
+                       const std::vector<uint32_t> &seed_rows, KMeansBufs &kb, DevBuf &block, int32_t *lab,
+                       float *best, __nv_bfloat16 **centb_out) {
+    cudaError_t e;
+    const uint32_t brows = (uint32_t)std::max<size_t>(1024, std::min<size_t>(65536, ((size_t)1 << 29) / C));
+    if ((e = kb.work.reserve((size_t)C * D * 4 * 2 + (size_t)C * D * 2 + (size_t)C * 8 + 64)) != cudaSuccess ||
+        (e = kb.rows.reserve((size_t)C * 4)) != cudaSuccess || (e = block.reserve((size_t)brows * C * 4)) != cudaSuccess)
+        return e;
+    float *cent = kb.work.as<float>();
+    float *csum = cent + (size_t)C * D;
+    __nv_bfloat16 *centb = reinterpret_cast<__nv_bfloat16 *>(csum + (size_t)C * D);
+    float *cn = reinterpret_cast<float *>(centb + (size_t)C * D);
+    uint32_t *ccnt = reinterpret_cast<uint32_t *>(cn + C);
+    cudaMemcpyAsync(kb.rows.p, seed_rows.data(), (size_t)C * 4, cudaMemcpyHostToDevice, st);
+    init_centroids_kernel<<<blocks_for((size_t)C * D), 256, 0, st>>>(F, D, kb.rows.as<uint32_t>(), C, cent);
+    cudaMemsetAsync(ccnt, 0, (size_t)C * 4, st);
+    kmeans_update_kernel<<<C, 128, 0, st>>>(cent, csum, ccnt, C, D, centb, cn);
+    for (uint32_t it = 0; it <= iters; ++it) {
+        for (uint32_t r0 = 0; r0 < n; r0 += brows) {
+            const uint32_t rows = std::min<uint32_t>(brows, n - r0);
+            gemm(st, rows, C, D, F + (size_t)r0 * D, D, 0, centb, D, 1, block.as<float>(), C, nullptr, nullptr, 0);
+            argmin_kernel<<<(rows * 32 + 255) / 256, 256, 0, st>>>(block.as<float>(), cn, rows, C, lab + r0, best + r0);
+        }
+        if (it == iters) break;
+        cudaMemsetAsync(csum, 0, (size_t)C * D * 4, st);
+        cudaMemsetAsync(ccnt, 0, (size_t)C * 4, st);
+        kmeans_accumulate_kernel<<<blocks_for((size_t)n * D), 256, 0, st>>>(F, lab, n, D, csum, ccnt);
+        kmeans_update_kernel<<<C, 128, 0, st>>>(cent, csum, ccnt, C, D, centb, cn);
+    }
+    *centb_out = centb;
+    return cudaGetLastError();
+}
+
+constexpr uint32_t MIN_COMPONENT = 8;
+constexpr size_t LABEL_CHUNKS = 16;   // label searches, each with its own seeds
+
+// Component label of every node of the context's graph (host copy in comp).
+int graph_components(kg_ctx *ctx, DevBuf &buf, std::vector<uint32_t> &comp) {
+    const uint32_t N = ctx->gn;
+    cudaStream_t st = ctx->stream;
+    cudaError_t e;
+    if ((e = buf.reserve((size_t)N * 4 + 16)) != cudaSuccess) return cuda_fail(ctx, e, "router alloc");
+    uint32_t *lab = buf.as<uint32_t>(), *changed = lab + N;
+    iota_kernel<<<blocks_for(N), 256, 0, st>>>(N, lab);
+    for (int it = 0; it < 1000; ++it) {
+        uint32_t h = 0;
+        cudaMemsetAsync(changed, 0, 4, st);
+        cc_hook_kernel<<<blocks_for((size_t)N * 32), 256, 0, st>>>(N, ctx->offsets.as<uint64_t>(),
+                                                                   ctx->nbr.as<uint32_t>(), lab, changed);
+        cc_jump_kernel<<<blocks_for(N), 256, 0, st>>>(N, lab);
+        cudaMemcpyAsync(&h, changed, 4, cudaMemcpyDeviceToHost, st);
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "graph components");
+        if (!h) break;
+    }
+    comp.resize(N);
+    cudaMemcpyAsync(comp.data(), lab, (size_t)N * 4, cudaMemcpyDeviceToHost, st);
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "graph components");
+    return KG_OK;
+}
+
 void init_weights(RouterState &r, uint64_t seed) {
     std::mt19937_64 rng(seed);
     const uint32_t in[3] = {r.D, r.H, r.H}, out[3] = {r.H, r.H, r.C};
@@ -422,6 +611,10 @@ extern "C" void kg_router_params_default(kg_router_params *p) {
     p->batch = 1024;
     p->lr = 2e-3f;
     p->seed = 1998;
+    p->entries = 8;
+    p->probe = 8;
+    p->refine = 2;
+    p->refine_P = 50;
 }
 
 extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const float *train_queries, size_t ntrain,
@@ -431,21 +624,35 @@ extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const flo
     {
         Guard g(ctx);
         if (!ctx->has_data || !ctx->has_graph) return set_error(ctx, KG_E_RUNTIME, "router needs a dataset and a graph");
-        if (p->clusters < 2 || p->clusters > 2048 || p->hidden < 8 || p->batch < 1)
-            return set_error(ctx, KG_E_INVALID, "router sizes out of range (clusters 2..2048)");
+        if (p->clusters < 2 || p->clusters > 2048 || p->hidden < 8 || p->batch < 1 || p->entries > 16 ||
+            p->probe < 1 || p->probe > 32 || p->refine > 8)
+            return set_error(ctx, KG_E_INVALID, "router sizes out of range (clusters 2..2048, entries 0..16, "
+                                                "probe 1..32)");
     }
-    // 1. labels: the best node the plain search finds for each training query
+    // 1. labels: the best node the plain search finds for each training query.
+    //    The plain search starts every query of a call from the same P seeds
+    //    (kgraph.cpp:444-453), so a region without a seed is missed by every
+    //    query of the call; the training queries are therefore searched in
+    //    LABEL_CHUNKS calls with different seeds, which spreads those misses
+    //    over different regions instead of repeating them.
     std::vector<uint32_t> top(ntrain), cnt(ntrain);
-    {
+    std::vector<float> topd(ntrain);
+    for (size_t c = 0; c < LABEL_CHUNKS; ++c) {
+        const size_t a = ntrain * c / LABEL_CHUNKS, b = ntrain * (c + 1) / LABEL_CHUNKS;
+        if (a == b) continue;
         kg_search_params sp;
         kg_search_params_default(&sp);
         sp.K = 1;
         sp.P = p->label_P;
-        int rc = kg_search_batch(ctx, train_queries, ntrain, q_stride_bytes, &sp, nullptr, nullptr, 1, top.data(),
-                                 nullptr, cnt.data(), nullptr);
+        sp.seed = p->seed + 1 + (unsigned)c;
+        const float *qa = reinterpret_cast<const float *>(reinterpret_cast<const char *>(train_queries) +
+                                                          a * q_stride_bytes);
+        int rc = kg_search_batch(ctx, qa, b - a, q_stride_bytes, &sp, nullptr, nullptr, 1, top.data() + a,
+                                 topd.data() + a, cnt.data() + a, nullptr);
         if (rc != KG_OK) return rc;
     }
-    Guard g(ctx);
+    std::unique_lock<std::mutex> lk(ctx->mu);   // released around the refinement's searches
+    cudaSetDevice(ctx->device);
     cudaStream_t st = ctx->stream;
     cudaError_t e;
     if (!ctx->router) ctx->router = new RouterState;
@@ -468,67 +675,97 @@ extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const flo
     for (size_t i = 0; i < (size_t)N * D; ++i) { double t = hX[i] - mu[i % D]; var[i % D] += t * t; }
     std::vector<float> hm(D), hs(D);
     for (uint32_t j = 0; j < D; ++j) { hm[j] = (float)mu[j]; hs[j] = (float)(1.0 / std::sqrt(var[j] / N + 1e-6)); }
-    if ((e = r.mean.reserve(D * 4)) != cudaSuccess || (e = r.inv_std.reserve(D * 4)) != cudaSuccess ||
-        (e = r.entry.reserve(C * 4)) != cudaSuccess)
+    if ((e = r.mean.reserve(D * 4)) != cudaSuccess || (e = r.inv_std.reserve(D * 4)) != cudaSuccess)
         return cuda_fail(ctx, e, "router alloc");
     cudaMemcpyAsync(r.mean.p, hm.data(), D * 4, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(r.inv_std.p, hs.data(), D * 4, cudaMemcpyHostToDevice, st);
 
-    // 3. k-means of the dataset features: C centroids from random members
+    // 3. entry clusters.  Fine level: k-means of the dataset features into
+    //    Cf = C x E clusters, entry node = the member nearest each centroid.
+    const uint32_t E = std::max(1u, p->entries), Cf = C * E;
     if ((e = s0.reserve((size_t)N * D * 2)) != cudaSuccess ||            // features (BF16)
-        (e = s1.reserve((size_t)C * D * 4 * 2 + (size_t)C * D * 2 + C * 8)) != cudaSuccess ||   // cent, sum, centb, cn, cnt
-        (e = s2.reserve((size_t)N * 4 * 2)) != cudaSuccess ||              // labels, best
-        (e = s3.reserve((size_t)65536 * C * 4)) != cudaSuccess)            // one block of X.C^T
+        (e = s2.reserve((size_t)N * 4 * 2 + (size_t)Cf * 8)) != cudaSuccess)   // labels, best (+ fine level's)
         return cuda_fail(ctx, e, "router alloc");
     __nv_bfloat16 *F = s0.as<__nv_bfloat16>();
-    float *cent = s1.as<float>();
-    float *csum = cent + (size_t)C * D;
-    __nv_bfloat16 *centb = reinterpret_cast<__nv_bfloat16 *>(csum + (size_t)C * D);
-    float *cn = reinterpret_cast<float *>(centb + (size_t)C * D);
-    uint32_t *ccnt = reinterpret_cast<uint32_t *>(cn + C);
     int32_t *lab = s2.as<int32_t>();
     float *best = reinterpret_cast<float *>(lab + N);
+    int32_t *labc = reinterpret_cast<int32_t *>(best + N);
+    float *bestc = reinterpret_cast<float *>(labc + Cf);
     features_kernel<<<blocks_for((size_t)N * D), 256, 0, st>>>(ctx->X.as<float>(), ctx->ld, nullptr, N, D,
                                                                  r.mean.as<float>(), r.inv_std.as<float>(), F);
+    KMeansBufs fine, coarse;
+    __nv_bfloat16 *centf = nullptr, *centc = nullptr;
+    std::mt19937 krng(p->seed);
     {
-        std::mt19937 rng(p->seed);
-        std::vector<uint32_t> pick(C);
-        for (uint32_t c = 0; c < C; ++c) pick[c] = rng() % N;
-        std::vector<float> hc((size_t)C * D);
-        for (uint32_t c = 0; c < C; ++c)
-            for (uint32_t j = 0; j < D; ++j) hc[(size_t)c * D + j] = (hX[(size_t)pick[c] * D + j] - hm[j]) * hs[j];
-        cudaMemcpyAsync(cent, hc.data(), (size_t)C * D * 4, cudaMemcpyHostToDevice, st);
-        cudaMemsetAsync(ccnt, 0, C * 4, st);
-        kmeans_update_kernel<<<C, 128, 0, st>>>(cent, csum, ccnt, C, D, centb, cn);
+        std::vector<uint32_t> pick(Cf);
+        for (uint32_t c = 0; c < Cf; ++c) pick[c] = krng() % N;
+        if ((e = kmeans_run(st, F, N, D, Cf, p->kmeans_iters, pick, fine, s3, lab, best, &centf)) != cudaSuccess)
+            return cuda_fail(ctx, e, "router kmeans");
     }
-    for (uint32_t it = 0; it <= p->kmeans_iters; ++it) {
-        for (uint32_t r0 = 0; r0 < N; r0 += 65536) {
-            const uint32_t rows = std::min<uint32_t>(65536, N - r0);
-            gemm(st, rows, C, D, F + (size_t)r0 * D, D, 0, centb, D, 1, s3.as<float>(), C, nullptr, nullptr, 0);
-            argmin_kernel<<<(rows * 32 + 255) / 256, 256, 0, st>>>(s3.as<float>(), cn, rows, C, lab + r0, best + r0);
-        }
-        if (it == p->kmeans_iters) break;
-        cudaMemsetAsync(csum, 0, (size_t)C * D * 4, st);
-        cudaMemsetAsync(ccnt, 0, C * 4, st);
-        kmeans_accumulate_kernel<<<blocks_for((size_t)N * D), 256, 0, st>>>(F, lab, N, D, csum, ccnt);
-        kmeans_update_kernel<<<C, 128, 0, st>>>(cent, csum, ccnt, C, D, centb, cn);
-    }
-    // entry node per cluster (nearest member; an empty cluster points at node 0)
-    unsigned long long *key = reinterpret_cast<unsigned long long *>(s3.p);
-    cudaMemsetAsync(key, 0xFF, C * 8, st);
+    unsigned long long *key = reinterpret_cast<unsigned long long *>(s1.p);
+    if ((e = s1.reserve((size_t)Cf * 8)) != cudaSuccess) return cuda_fail(ctx, e, "router alloc");
+    key = reinterpret_cast<unsigned long long *>(s1.p);
+    cudaMemsetAsync(key, 0xFF, (size_t)Cf * 8, st);
     entry_kernel<<<blocks_for(N), 256, 0, st>>>(lab, best, N, key);
-    std::vector<unsigned long long> hkey(C);
-    std::vector<int32_t> hlab(N);
-    cudaMemcpyAsync(hkey.data(), key, C * 8, cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(hlab.data(), lab, (size_t)N * 4, cudaMemcpyDeviceToHost, st);
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "router kmeans");
-    std::vector<uint32_t> hentry(C);
-    uint32_t empty = 0;
-    for (uint32_t c = 0; c < C; ++c) {
-        if (hkey[c] == ~0ull) { hentry[c] = 0; ++empty; }
-        else hentry[c] = (uint32_t)(hkey[c] & 0xFFFFFFFFu);
+    // Coarse level: the fine centroids grouped into the C clusters of the MLP.
+    if (E > 1) {
+        std::vector<uint32_t> pick(C);
+        for (uint32_t c = 0; c < C; ++c) pick[c] = krng() % Cf;
+        if ((e = kmeans_run(st, centf, Cf, D, C, p->kmeans_iters, pick, coarse, s3, labc, bestc, &centc)) !=
+            cudaSuccess)
+            return cuda_fail(ctx, e, "router kmeans");
     }
-    cudaMemcpyAsync(r.entry.p, hentry.data(), C * 4, cudaMemcpyHostToDevice, st);
+    std::vector<unsigned long long> hkey(Cf);
+    std::vector<int32_t> hlab(N), hlabc(Cf);
+    cudaMemcpyAsync(hkey.data(), key, (size_t)Cf * 8, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hlab.data(), lab, (size_t)N * 4, cudaMemcpyDeviceToHost, st);
+    if (E > 1) cudaMemcpyAsync(hlabc.data(), labc, (size_t)Cf * 4, cudaMemcpyDeviceToHost, st);
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "router kmeans");
+    if (E == 1)
+        for (uint32_t f = 0; f < Cf; ++f) hlabc[f] = (int32_t)f;
+    // the cluster of every node (coarse label of its fine cluster)
+    for (uint32_t i = 0; i < N; ++i) hlab[i] = hlabc[hlab[i]];
+    // Entry nodes per cluster: those of its non-empty fine clusters, plus one
+    // node of every connected component of the graph (of at least
+    // MIN_COMPONENT nodes) that holds no fine entry node: a walk never leaves
+    // its component, so every component needs a way in.  Such a node joins the
+    // cluster its own members are assigned to.
+    std::vector<std::pair<uint32_t, uint32_t>> ent;   // (cluster, node)
+    ent.reserve(Cf + 1024);
+    for (uint32_t f = 0; f < Cf; ++f)
+        if (hkey[f] != ~0ull) ent.emplace_back((uint32_t)hlabc[f], (uint32_t)(hkey[f] & 0xFFFFFFFFu));
+    uint32_t comp_entries = 0;
+    {
+        std::vector<uint32_t> comp;
+        int rc = graph_components(ctx, s1, comp);
+        if (rc != KG_OK) return rc;
+        std::vector<uint32_t> size(N, 0);
+        std::vector<uint8_t> covered(N, 0);
+        for (uint32_t i = 0; i < ctx->gn; ++i) ++size[comp[i]];
+        for (auto &pr : ent) covered[comp[pr.second]] = 1;
+        for (uint32_t i = 0; i < ctx->gn; ++i)
+            if (comp[i] == i && !covered[i] && size[i] >= MIN_COMPONENT) {   // i: the component's smallest id
+                ent.emplace_back((uint32_t)hlab[i], i);
+                ++comp_entries;
+            }
+    }
+    std::stable_sort(ent.begin(), ent.end(),
+                     [](const std::pair<uint32_t, uint32_t> &a, const std::pair<uint32_t, uint32_t> &b) {
+                         return a.first < b.first;
+                     });
+    std::vector<uint32_t> heoff(C + 1, 0), heids(ent.size());
+    for (size_t k = 0; k < ent.size(); ++k) { ++heoff[ent[k].first + 1]; heids[k] = ent[k].second; }
+    for (uint32_t c = 0; c < C; ++c) heoff[c + 1] += heoff[c];
+    uint32_t empty = 0;   // clusters without an entry node
+    for (uint32_t c = 0; c < C; ++c) empty += heoff[c + 1] == heoff[c];
+    if ((e = r.eoff.reserve((size_t)(C + 1) * 4)) != cudaSuccess ||
+        (e = r.eids.reserve(std::max<size_t>(heids.size(), 1) * 4)) != cudaSuccess)
+        return cuda_fail(ctx, e, "router alloc");
+    cudaMemcpyAsync(r.eoff.p, heoff.data(), (size_t)(C + 1) * 4, cudaMemcpyHostToDevice, st);
+    if (!heids.empty()) cudaMemcpyAsync(r.eids.p, heids.data(), heids.size() * 4, cudaMemcpyHostToDevice, st);
+    r.probe = std::max(1u, std::min(p->probe, C));
+    r.entries_total = (uint32_t)heids.size();
+    r.component_entries = comp_entries;
 
     // 4. training set: query features and the cluster of each query's best node
     std::vector<int32_t> ylab(ntrain);
@@ -547,7 +784,8 @@ extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const flo
     unsigned step = 0;
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
     const size_t full = ntrain < B ? ntrain : ntrain / B * B;   // the last partial batch is dropped
-    for (uint32_t ep = 0; ep < p->epochs; ++ep) {
+    auto run_epochs = [&](uint32_t epochs) -> int {
+    for (uint32_t ep = 0; ep < epochs; ++ep) {
         std::shuffle(order.begin(), order.end(), rng);
         for (size_t s0i = 0; s0i < full; s0i += B) {
             const uint32_t bs = (uint32_t)std::min<size_t>(B, full - s0i);
@@ -580,6 +818,48 @@ extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const flo
             last_loss = hl / bs;
         }
     }
+    return KG_OK;
+    };
+    int rc0 = run_epochs(p->epochs);
+    if (rc0 != KG_OK) return rc0;
+    // 5. refinement: the router's own seeds, handed to the walk, may find a
+    //    closer node than the plain search did for a training query; the closer
+    //    of the two becomes its label and training continues.
+    std::vector<uint32_t> sids, scnt;
+    std::vector<float> sd;
+    unsigned relabelled = 0;
+    for (uint32_t round = 0; round < p->refine; ++round) {
+        r.trained = true;
+        const unsigned m = 3, ld = m + 1;   // the reference requires init < K
+        sids.assign(ntrain * ld, 0u);
+        scnt.assign(ntrain, 0u);
+        sd.assign(ntrain * ld, 0.f);
+        lk.unlock();
+        int rc = kg_router_seeds(ctx, train_queries, ntrain, q_stride_bytes, m, sids.data(), ld);
+        if (rc == KG_OK) {
+            kg_search_params sp;
+            kg_search_params_default(&sp);
+            sp.K = ld;
+            sp.P = p->refine_P;
+            sp.init = m;
+            rc = kg_search_batch(ctx, train_queries, ntrain, q_stride_bytes, &sp, nullptr, nullptr, ld, sids.data(),
+                                 sd.data(), scnt.data(), nullptr);
+        }
+        lk.lock();
+        cudaSetDevice(ctx->device);
+        if (rc != KG_OK) return rc;
+        for (size_t i = 0; i < ntrain; ++i) {
+            if (!scnt[i] || (cnt[i] && !(sd[i * ld] < topd[i]))) continue;
+            const uint32_t node = sids[i * ld];
+            if (node >= N) continue;
+            if (!cnt[i] || hlab[node] != ylab[i]) ++relabelled;
+            top[i] = node;
+            topd[i] = sd[i * ld];
+            cnt[i] = 1;
+            ylab[i] = hlab[node];
+        }
+        if ((rc = run_epochs(p->epochs)) != KG_OK) return rc;
+    }
     // accuracy of the final weights on the first min(ntrain, 4096) training rows
     float acc = 0.f;
     {
@@ -609,6 +889,9 @@ extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const flo
         info->final_loss = last_loss;
         info->train_accuracy = acc;
         info->empty_clusters = empty;
+        info->entries = r.entries_total;
+        info->component_entries = r.component_entries;
+        info->relabelled = relabelled;
     }
     return check_device_error(ctx, "router");
 }
@@ -625,6 +908,14 @@ extern "C" int kg_router_seeds(kg_ctx *ctx, const float *queries, size_t nq, siz
     DevBuf &tq = ctx->build_scratch[19], &out = ctx->build_scratch[18];
     const bool sdev = is_device_ptr(seeds);
     if (!sdev && (e = out.reserve(nq * out_ld * 4)) != cudaSuccess) return cuda_fail(ctx, e, "router alloc");
+    if ((e = r.topc.reserve((size_t)r.batch * r.probe * 4)) != cudaSuccess) return cuda_fail(ctx, e, "router alloc");
+    {
+        const size_t smem = (size_t)RANK_WARPS * (ctx->ld + 2 * RANK_CAND) * 4;
+        if (smem > 48 * 1024 &&
+            (e = cudaFuncSetAttribute(seed_rank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+                cudaSuccess)
+            return cuda_fail(ctx, e, "router seeds");
+    }
     uint32_t *dst = sdev ? seeds : out.as<uint32_t>();
     if (!sdev) cudaMemcpyAsync(dst, seeds, nq * out_ld * 4, cudaMemcpyHostToDevice, st);
     const char *qb = reinterpret_cast<const char *>(queries);
@@ -634,8 +925,15 @@ extern "C" int kg_router_seeds(kg_ctx *ctx, const float *queries, size_t nq, siz
         int rc = stage_queries(ctx, r, reinterpret_cast<const float *>(qb + c0 * q_stride_bytes), bs, q_stride_bytes, tq);
         if (rc != KG_OK) return rc;
         forward(st, r, (int)bs);
-        topm_kernel<<<((int)bs * 32 + 255) / 256, 256, 0, st>>>(r.Z.as<float>(), (int)bs, r.C, (int)m,
-                                                                 r.entry.as<uint32_t>(), dst + c0 * out_ld, (int)out_ld);
+        topm_kernel<<<((int)bs * 32 + 255) / 256, 256, 0, st>>>(r.Z.as<float>(), (int)bs, r.C, (int)r.probe, nullptr,
+                                                                 r.topc.as<uint32_t>(), (int)r.probe);
+        const DataView DV{ctx->X.as<float>(), ctx->norms.as<float>(), ctx->n, ctx->d, ctx->ld, ctx->metric};
+        const size_t smem = (size_t)RANK_WARPS * (ctx->ld + 2 * RANK_CAND) * 4;
+        const int grid = (int)std::min<size_t>((bs + RANK_WARPS - 1) / RANK_WARPS, (size_t)ctx->num_sms * 8);
+        seed_rank_kernel<<<grid, RANK_WARPS * 32, smem, st>>>(DV, tq.as<float>(), (int)bs, r.topc.as<uint32_t>(),
+                                                               (int)r.probe, r.eoff.as<uint32_t>(),
+                                                               r.eids.as<uint32_t>(), (int)m, dst + c0 * out_ld,
+                                                               (int)out_ld);
     }
     cudaEventRecord(ctx->ev1, st);
     if (!sdev) cudaMemcpyAsync(seeds, dst, nq * out_ld * 4, cudaMemcpyDeviceToHost, st);
