@@ -133,6 +133,38 @@ int kg_search_autotune(kg_ctx *ctx, const float *queries, size_t nq, size_t q_st
 int kg_set_search_tuning(kg_ctx *ctx, const kg_search_tuning *t);
 int kg_get_search_tuning(kg_ctx *ctx, kg_search_tuning *t);
 
+/* Distance filter of the search.  No counterpart in the reference (its walk
+ * evaluates every candidate in FP32, kgraph.cpp:495-513).  With BF16 or FP8
+ * (E4M3 with a per-row scale), the walk first evaluates each candidate against
+ * a compressed copy of its row and derives a rigorous lower bound of its
+ * canonical FP32 distance (FP32 accumulation, the copy's per-row error bound and
+ * the FP32 rounding bounds of both computations).  Once the pool is full, a
+ * candidate whose bound is at or beyond the pool's last entry -- one the
+ * reference would drop into the spare slot -- is not evaluated in FP32; every
+ * other candidate is, exactly as without the filter.  Results (ids,
+ * distances, counts, costs) are identical in every mode.  The copy is built on
+ * the call (and again after kg_set_data), n * round_up(d, 16) * 2 (BF16) or
+ * * 1 (FP8) bytes plus 16 bytes per row. */
+enum { KG_SEARCH_FP32 = 0, KG_SEARCH_BF16 = 1, KG_SEARCH_FP8 = 2 };
+int kg_set_search_precision(kg_ctx *ctx, int mode);
+/* The filter's work in the last kg_search_batch and its copy's quantisation
+ * error: approx = candidates evaluated on the compressed rows, skipped = of
+ * those, the ones the bound excluded (FP32 evaluations saved); max / mean over
+ * rows of ||x - y|| / ||x||, y the reconstructed row. */
+typedef struct {
+    int mode;
+    unsigned long long approx, skipped;
+    double max_rel_row_error, mean_rel_row_error;
+} kg_search_filter_stats;
+int kg_last_search_filter(kg_ctx *ctx, kg_search_filter_stats *out);
+/* Check of the filter's arithmetic: for each of nq queries and each of its
+ * per_query dataset rows (ids, nq rows of per_query), the lower bound the
+ * filter derives from the compressed row (lb) and the canonical FP32 distance
+ * (dist); lb <= dist must hold for every pair.  Needs a BF16 or FP8 search
+ * precision and d <= 256.  Pointers may be host or device memory. */
+int kg_filter_bounds(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes, const uint32_t *ids,
+                     size_t per_query, float *lb, float *dist);
+
 /* KGraphImpl::reverse (kgraph.cpp:667-702) on the current graph. */
 int kg_reverse(kg_ctx *ctx, int rev_k);
 /* KGraph::prune (kgraph.h:180; kgraph.cpp:584-665) on the current graph. */

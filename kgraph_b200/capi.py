@@ -22,7 +22,8 @@ SYMBOLS = [
     "kg_last_search_work", "kg_search_batch_noalloc", "kg_noalloc_scratch_bytes",
     "kg_router_params_default", "kg_router_train", "kg_router_seeds", "kg_router_gradients", "kg_last_router_timing",
     "kg_set_join_precision", "kg_last_join_stats", "kg_last_build_graphs", "kg_search_autotune",
-    "kg_set_search_tuning", "kg_get_search_tuning",
+    "kg_set_search_tuning", "kg_get_search_tuning", "kg_set_search_precision", "kg_last_search_filter",
+    "kg_filter_bounds",
 ]
 
 JOIN = {"auto": 0, "fp32": 1, "bf16": 2, "bf16_always": 3}
@@ -62,6 +63,14 @@ class JoinStats(C.Structure):
 class SearchTuning(C.Structure):
     _fields_ = [("split", C.c_uint), ("warps_per_block", C.c_uint), ("prefetch", C.c_uint), ("ms", C.c_float),
                 ("default_ms", C.c_float), ("variants", C.c_uint)]
+
+
+class FilterStats(C.Structure):
+    _fields_ = [("mode", C.c_int), ("approx", C.c_ulonglong), ("skipped", C.c_ulonglong),
+                ("max_rel_row_error", C.c_double), ("mean_rel_row_error", C.c_double)]
+
+
+SEARCH_PRECISION = {"fp32": 0, "bf16": 1, "fp8": 2}
 
 
 class SearchParams(C.Structure):
@@ -111,6 +120,9 @@ def lib():
                                          C.POINTER(SearchTuning)]
         L.kg_set_search_tuning.argtypes = [vp, C.POINTER(SearchTuning)]
         L.kg_get_search_tuning.argtypes = [vp, C.POINTER(SearchTuning)]
+        L.kg_set_search_precision.argtypes = [vp, C.c_int]
+        L.kg_last_search_filter.argtypes = [vp, C.POINTER(FilterStats)]
+        L.kg_filter_bounds.argtypes = [vp, vp, sz, sz, vp, sz, vp, vp]
         L.kg_index_params_default.argtypes = [C.POINTER(IndexParams)]
         L.kg_search_params_default.argtypes = [C.POINTER(SearchParams)]
         _lib = L
@@ -310,6 +322,28 @@ class Context:
         t = SearchTuning()
         self._check(self.L.kg_get_search_tuning(self.h, C.byref(t)))
         return {"split": t.split, "warps_per_block": t.warps_per_block, "prefetch": t.prefetch}
+
+    def set_search_precision(self, mode):
+        """'fp32' (default), 'bf16' or 'fp8': compressed rows that filter the walk's candidates."""
+        self._check(self.L.kg_set_search_precision(self.h, SEARCH_PRECISION[mode] if isinstance(mode, str)
+                                                    else int(mode)))
+
+    def search_filter_stats(self):
+        st = FilterStats()
+        self._check(self.L.kg_last_search_filter(self.h, C.byref(st)))
+        out = {f: getattr(st, f) for f, _ in FilterStats._fields_}
+        out["mode"] = {0: "fp32", 1: "bf16", 2: "fp8"}[st.mode]
+        return out
+
+    def filter_bounds(self, Q, ids):
+        """(lower bound, canonical distance) of every (query, ids[q, j]) pair."""
+        Q = np.ascontiguousarray(Q, np.float32)
+        ids = np.ascontiguousarray(ids, np.uint32)
+        lb = np.zeros(ids.shape, np.float32)
+        dist = np.zeros(ids.shape, np.float32)
+        self._check(self.L.kg_filter_bounds(self.h, _ptr(Q), Q.shape[0], Q.strides[0], _ptr(ids), ids.shape[1],
+                                            _ptr(lb), _ptr(dist)))
+        return lb, dist
 
     def build_graph_launches(self):
         """CUDA graph launches of the last build's iterations."""

@@ -201,6 +201,11 @@ int kg_set_data(kg_ctx *ctx, const float *rows, size_t n, size_t d, size_t strid
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "norms");
     if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "set_data");
     ctx->has_data = true;
+    ++ctx->data_version;
+    if (ctx->search_prec != KG_SEARCH_FP32) {
+        int r = ensure_search_precision(ctx);
+        if (r != KG_OK) return r;
+    }
     // A graph from another dataset is not valid for this one.
     if (ctx->has_graph && ctx->gn > ctx->n) ctx->has_graph = false;
     return KG_OK;
@@ -462,7 +467,14 @@ int search_locked(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_
     a.qcounter = ctx->counter.as<uint32_t>();
     a.err = ctx->errw.as<uint32_t>();
     a.work = reinterpret_cast<unsigned long long *>(ctx->counter.as<char>() + 16);
-    cudaMemsetAsync(ctx->counter.p, 0, 32, ctx->stream);
+    cudaMemsetAsync(ctx->counter.p, 0, 48, ctx->stream);
+    if (graph && ctx->search_prec != KG_SEARCH_FP32) {
+        int pr = ensure_search_precision(ctx);
+        if (pr != KG_OK) return pr;
+        a.prec = (uint32_t)ctx->search_prec;
+        a.Xc = ctx->Xc.p;
+        a.cmeta = ctx->cmeta.as<float4>();
+    }
 
     cudaEventRecord(ctx->ev0, ctx->stream);
     if ((e = launch_search(a, sh, ctx->num_sms, ctx->stream, nullptr)) != cudaSuccess)
@@ -473,7 +485,7 @@ int search_locked(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_
     if (dists && !d_dev) cudaMemcpyAsync(dists, a.out_dists, Q * out_ld * 4, cudaMemcpyDeviceToHost, ctx->stream);
     if (!c_dev) cudaMemcpyAsync(counts, a.out_count, Q * 4, cudaMemcpyDeviceToHost, ctx->stream);
     if (costs && !cost_dev) cudaMemcpyAsync(costs, a.out_cost, Q * 4, cudaMemcpyDeviceToHost, ctx->stream);
-    cudaMemcpyAsync(ctx->last_work, a.work, 16, cudaMemcpyDeviceToHost, ctx->stream);
+    cudaMemcpyAsync(ctx->last_work, a.work, 32, cudaMemcpyDeviceToHost, ctx->stream);
     if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "search");
     cudaEventElapsedTime(&ctx->last_search_ms, ctx->ev0, ctx->ev1);
     return check_device_error(ctx, "search");

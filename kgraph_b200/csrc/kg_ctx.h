@@ -48,13 +48,20 @@ struct kg_ctx {
     std::string err;
     float last_build_ms = 0.f, last_search_ms = 0.f, last_router_ms = 0.f;
     unsigned last_build_graph_launches = 0;   // CUDA graph launches of the last build's iterations
-    unsigned long long last_work[2] = {0, 0};
+    unsigned long long last_work[4] = {0, 0, 0, 0};   // evaluations, adjacency reads, filter: approx, skipped
 
     // dataset
     kgb::DevBuf X, norms;
     uint32_t n = 0, d = 0, ld = 0;
     int metric = 0;
     bool has_data = false;
+    uint64_t data_version = 0;       // bumped whenever the dataset changes
+
+    // reduced-precision copy for the search's distance filter (kg_precision.cu)
+    int search_prec = KG_SEARCH_FP32, prec_built = KG_SEARCH_FP32;
+    uint64_t prec_data_version = ~0ull;
+    kgb::DevBuf Xc, cmeta, cstats;
+    double prec_max_rel = 0.0, prec_mean_rel = 0.0;
 
     // graph, CSR
     kgb::DevBuf offsets, nbr, nbr_d, Mnode;
@@ -91,6 +98,8 @@ int cuda_fail(kg_ctx *ctx, cudaError_t e, const char *what);
 bool is_device_ptr(const void *p);
 // Reads and clears the device error word; returns KG_OK or sets the message.
 int check_device_error(kg_ctx *ctx, const char *what);
+// Builds the compressed rows of ctx->search_prec if the dataset changed since.
+int ensure_search_precision(kg_ctx *ctx);
 // Exact top-K brute force of `nq` dataset rows (LinearSearch, kgraph.cpp:212-229)
 // used for the build's control nodes.
 cudaError_t launch_linear_search(kg_ctx *ctx, const uint32_t *rows, uint32_t nq, uint32_t K, uint32_t *out_ids,

@@ -17,6 +17,8 @@
 // pure), then inserted one by one in order, which is what the reference's
 // interleaved loop produces.  With the canonical distance this reproduces
 // the reference's ids, distances, result count and SearchInfo.cost exactly.
+#include <cuda_fp16.h>
+#include <cuda_fp8.h>
 #include <algorithm>
 #include "kg_common.cuh"
 #include "kg_warp.cuh"
@@ -162,11 +164,139 @@ __device__ __forceinline__ bool visited_test_set(uint32_t *vis, uint32_t id) {
     return (old & bit) != 0;
 }
 
+// ---- the distance filter on compressed rows (kg_precision.cu) ----
+constexpr float U32 = 5.9604645e-8f;   // unit roundoff of FP32, 2^-24
+
+// The W reconstructed values of `row` at elements [off, off + W): BF16 values,
+// or FP8 E4M3 values times the row's scale (rounded to FP32, as the error
+// bound of the compressed row assumes).
+template <int PREC, int W>
+__device__ __forceinline__ void load_y(const void *Xc, uint32_t ld, uint32_t row, uint32_t off, float scale,
+                                       float *y) {
+    if constexpr (PREC == 1) {
+        const uint16_t *p = reinterpret_cast<const uint16_t *>(Xc) + (size_t)row * ld + off;
+        uint32_t w[W / 2];
+        if constexpr (W == 8) { const uint4 v = *reinterpret_cast<const uint4 *>(p); w[0] = v.x; w[1] = v.y; w[2] = v.z; w[3] = v.w; }
+        else if constexpr (W == 4) { const uint2 v = *reinterpret_cast<const uint2 *>(p); w[0] = v.x; w[1] = v.y; }
+        else { w[0] = *reinterpret_cast<const uint32_t *>(p); }
+#pragma unroll
+        for (int j = 0; j < W / 2; ++j) {
+            y[2 * j] = __uint_as_float(w[j] << 16);
+            y[2 * j + 1] = __uint_as_float(w[j] & 0xFFFF0000u);
+        }
+    } else {
+        const uint8_t *p = reinterpret_cast<const uint8_t *>(Xc) + (size_t)row * ld + off;
+        uint16_t h[W / 2];
+        if constexpr (W == 8) {
+            const uint2 v = *reinterpret_cast<const uint2 *>(p);
+            h[0] = (uint16_t)v.x; h[1] = (uint16_t)(v.x >> 16); h[2] = (uint16_t)v.y; h[3] = (uint16_t)(v.y >> 16);
+        } else if constexpr (W == 4) {
+            const uint32_t v = *reinterpret_cast<const uint32_t *>(p);
+            h[0] = (uint16_t)v; h[1] = (uint16_t)(v >> 16);
+        } else {
+            h[0] = *reinterpret_cast<const uint16_t *>(p);
+        }
+#pragma unroll
+        for (int j = 0; j < W / 2; ++j) {
+            const __half2_raw r = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)h[j], __NV_E4M3);
+            const float2 f = __half22float2(__half2(r));
+            y[2 * j] = __fmul_rn(f.x, scale);
+            y[2 * j + 1] = __fmul_rn(f.y, scale);
+        }
+    }
+}
+
+// Sum over the row of (q - y)^2 (dot q.y for angular) with FP32 accumulation,
+// by the G-lane group of this lane; every lane of the group gets the sum.
+template <int PREC, int G>
+__device__ __forceinline__ float approx_raw(const SearchArgs &a, const float *q, uint32_t row, int t, float scale) {
+    constexpr int W = 16 / G;
+    const bool dot = a.D.metric == METRIC_ANGULAR;
+    float acc = 0.f;
+    const uint32_t chunks = a.D.ld >> 4;
+    for (uint32_t c = 0; c < chunks; ++c) {
+        const uint32_t off = 16 * c + W * t;
+        float y[W];
+        load_y<PREC, W>(a.Xc, a.D.ld, row, off, scale, y);
+#pragma unroll
+        for (int j = 0; j < W; ++j) {
+            const float qj = q[off + j];
+            if (dot) acc = __fmaf_rn(qj, y[j], acc);
+            else { const float df = __fsub_rn(qj, y[j]); acc = __fmaf_rn(df, df, acc); }
+        }
+    }
+#pragma unroll
+    for (int o = G / 2; o; o >>= 1) acc = __fadd_rn(acc, __shfl_xor_sync(FULL, acc, o));
+    return acc;
+}
+
+// Rigorous lower bound of the canonical FP32 distance (kg_common.cuh) of a row
+// x from `raw` (approx_raw over its reconstruction y, ||x - y|| <= e), the
+// query's and the row's norm terms nq, nx.  gamma_k = k u bounds the relative
+// error of a k-deep FP32 sum: ld + 8 deep for approx_raw, d/16 + 24 for the
+// canonical distance (16 lanes, a 4-level tree, up to 15 tail terms).  Every
+// step rounds towards the bound.
+__device__ __forceinline__ float filter_lb(int metric, float raw, float e, float nq, float nx, uint32_t d,
+                                           uint32_t ld) {
+    const float ga = (float)(ld + 8) * U32 * 1.01f;
+    const float gc = (float)(d / 16 + 24) * U32 * 1.01f;
+    if (metric == METRIC_ANGULAR) {
+        // -dot_c >= -dot' - ||q|| (e + ga ||y|| + gc ||x||);  ||q|| <= nq (1 + 2 gc), ||x|| <= nx (1 + 2 gc),
+        // ||y|| <= ||x|| + e; the canonical denominator is recomputed bit for bit, and rounding is monotone
+        const float qn = __fmul_ru(nq, 1.f + 2.f * gc);
+        const float xn = __fmul_ru(nx, 1.f + 2.f * gc);
+        const float yn = __fadd_ru(xn, e);
+        const float B = __fmul_ru(qn, __fadd_ru(e, __fadd_ru(__fmul_ru(ga, yn), __fmul_ru(gc, xn))));
+        const float num = __fsub_rd(-raw, B);
+        return __fdiv_rd(num, __fmaf_rn(nx, nq, FLT_EPSILON));
+    }
+    // ||q - y||^2 >= raw (1 - ga) and ||q - x|| >= ||q - y|| - e
+    const float r = __fsqrt_rd(fmaxf(__fmul_rd(raw, 1.f - ga), 0.f));
+    const float b = fmaxf(__fsub_rd(r, e), 0.f);
+    const float t2 = __fmul_rd(b, b);   // <= ||q - x||^2
+    if (metric == METRIC_L2SQR) return __fmul_rd(t2, 1.f - 2.f * gc);   // canonical >= ||q-x||^2 (1 - gamma)
+    // euclidean: canonical (n_q + n_x) - dot >= ||q - x||^2 / 2 - 2.2 gc (n_q + n_x)
+    return __fsub_rd(__fmul_rd(t2, 0.5f), __fmul_ru(2.2f * gc, __fadd_ru(nq, nx)));
+}
+
+// Lower bounds of the candidate lanes in `cm` from their compressed rows,
+// 32/G per pass; every candidate lane returns its own bound.
+template <int PREC, int G>
+__device__ __forceinline__ float warp_cand_lb(const SearchArgs &a, const float *q, float qn, unsigned cm, bool cand,
+                                              uint32_t id, int lane) {
+    constexpr uint32_t PER = 32 / G;
+    const int g = lane / G, t = lane % G;
+    const uint32_t n = __popc(cm);
+    const uint32_t my = __popc(cm & ((1u << lane) - 1u));
+    float mine = 0.f;
+    for (uint32_t base = 0; base < n; base += PER) {
+        const uint32_t i = base + g;
+        const int src = i < n ? (int)__fns(cm, 0, i + 1) : 0;
+        const uint32_t cid = __shfl_sync(FULL, id, src);
+        const uint32_t row = i < n ? cid : 0u;
+        const float4 md = a.cmeta[row];   // {error bound, scale, norm term, 0}
+        const float raw = approx_raw<PREC, G>(a, q, row, t, md.y);
+        const float lb = filter_lb(a.D.metric, raw, md.x, qn, md.z, a.D.d, a.D.ld);
+        const float got = __shfl_sync(FULL, lb, (int)(G * (my % PER)));
+        if (cand && my / PER == base / PER) mine = got;
+    }
+    return mine;
+}
+
+// L2 prefetch of a compressed row.
+template <int PREC>
+__device__ __forceinline__ void prefetch_crow(const SearchArgs &a, uint32_t id) {
+    const uint32_t bytes = a.D.ld * (PREC == 1 ? 2u : 1u);
+    const char *p = reinterpret_cast<const char *>(a.Xc) + (size_t)id * bytes;
+    for (uint32_t o = 0; o < bytes; o += 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(p + o));
+}
+
 }  // namespace
 
 // G: lanes per distance (the D-split, 32/G candidates per pass); PF: neighbour
-// batches whose rows are prefetched into L2 ahead of the walk.
-template <int G, int PF>
+// batches whose rows are prefetched into L2 ahead of the walk; PREC: 0, or the
+// compressed rows (1 BF16, 2 FP8) that filter candidates once the pool is full.
+template <int G, int PF, int PREC>
 __global__ void __launch_bounds__(256, 4) search_kernel(SearchArgs a) {
     extern __shared__ __align__(16) char smem[];
     const int lane = threadIdx.x & 31;
@@ -223,7 +353,7 @@ __global__ void __launch_bounds__(256, 4) search_kernel(SearchArgs a) {
             *reinterpret_cast<uint4 *>(vis + w) = make_uint4(0u, 0u, 0u, 0u);
         __syncwarp();
 
-        uint32_t n_comps = 0, n_adj = 0, n_seed = 0;
+        uint32_t n_comps = 0, n_adj = 0, n_seed = 0, n_apx = 0, n_skip = 0;
         uint32_t rn = 0;          // results.size() - 1
         bool have_results = false;
         for (uint32_t trial = 0; trial < T; ++trial) {
@@ -356,11 +486,42 @@ __global__ void __launch_bounds__(256, 4) search_kernel(SearchArgs a) {
 #pragma unroll
                             for (int cc = 0; cc < 4; ++cc) {
                                 const uint32_t pos = wlo + 32 * cc + lane;
-                                if (wuv[cc] && pos >= p1 && pos < p1 + PF * S && pos < whi)
-                                    prefetch_row(a.D, wid[cc]);
+                                if (wuv[cc] && pos >= p1 && pos < p1 + PF * S && pos < whi) {
+                                    if (PREC && L == cap - 1) prefetch_crow<PREC>(a, wid[cc]);
+                                    else prefetch_row(a.D, wid[cc]);
+                                }
                             }
                         }
-                        if (cm) {
+                        if (PREC && cm && L == cap - 1) {
+                            // Full pool: the visited test-and-set and the compressed rows in flight
+                            // together; the lower bound drops candidates that would land in the
+                            // spare slot, the others take the FP32 path below, restricted to them.
+                            bool isnew = false;
+                            if (cand) {
+                                const uint32_t bit = 1u << (id & 31);
+                                isnew = !(atomicOr(vis + (id >> 5), bit) & bit);
+                            }
+                            const float lb = warp_cand_lb<PREC, G>(a, s.q, qn, cm, cand, id, lane);
+                            const float worst = s.pd[L - 1];
+                            const bool keep = isnew && !(lb >= worst);
+                            const unsigned nm = __ballot_sync(FULL, isnew);
+                            const unsigned km = __ballot_sync(FULL, keep);
+                            n_comps += __popc(nm);
+                            n_apx += __popc(nm);
+                            n_skip += __popc(nm & ~km);
+                            if (km) {
+                                const uint32_t aM = keep ? actual_M(a, a.Mp, id) : 0u;
+                                const float dd = warp_cand_dist<G>(a, s.q, qn, km, keep, id, lane);
+                                const unsigned im = __ballot_sync(FULL, keep && dd < worst);
+                                if (im) {
+                                    uint32_t mr;
+                                    L = warp_batch_insert(s.pd, s.pid, s.pm, L, cap, im, dd, id | FLAG_BIT, aM << 16,
+                                                          &mr, lane);
+                                    if (mr <= k) moved = true;
+                                    if (mr < k) k = mr;
+                                }
+                            }
+                        } else if (cm) {
                             // All three in flight together: the exact test-and-set of the
                             // visited bit, the candidate's {M, degree}, and its row (distance).
                             bool isnew = false;
@@ -425,10 +586,54 @@ __global__ void __launch_bounds__(256, 4) search_kernel(SearchArgs a) {
             if (a.work) {
                 atomicAdd(a.work, (unsigned long long)(n_comps + n_seed));
                 atomicAdd(a.work + 1, (unsigned long long)n_adj);
+                if (PREC && n_apx) {
+                    atomicAdd(a.work + 2, (unsigned long long)n_apx);
+                    atomicAdd(a.work + 3, (unsigned long long)n_skip);
+                }
             }
         }
         __syncwarp();
     }
+}
+
+// The filter's lower bound and the canonical distance for `per` dataset rows
+// per query (one warp per query, one 4-lane group per row): the check of the
+// bound's arithmetic, lb <= dist for every pair.
+template <int PREC>
+__global__ void __launch_bounds__(256) filter_bounds_kernel(SearchArgs a, const uint32_t *ids, uint32_t per, float *lb,
+                                                            float *dist) {
+    __shared__ __align__(16) float qs[8][256];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t qi = blockIdx.x * 8 + w;
+    if (qi >= a.nq) return;   // whole warps
+    float *q = qs[w];
+    for (uint32_t x = lane; x < a.D.ld; x += 32) q[x] = a.Q[(size_t)qi * a.q_ld + x];
+    __syncwarp();
+    float qn = 0.f;
+    if (a.D.metric != METRIC_L2SQR) qn = norm_term(group4_raw(q, q, a.D.d, METRIC_EUCLIDEAN, lane & 3, FULL), a.D.metric);
+    const int g = lane >> 2, t = lane & 3;
+    for (uint32_t base = 0; base < per; base += 8) {
+        const uint32_t j = base + g;
+        const uint32_t row = j < per ? ids[(size_t)qi * per + j] : 0u;
+        const float4 md = a.cmeta[row];
+        const float raw = approx_raw<PREC, 4>(a, q, row, t, md.y);
+        const float b = filter_lb(a.D.metric, raw, md.x, qn, md.z, a.D.d, a.D.ld);
+        const float dd = query_dist(a.D, q, qn, row, t, FULL);
+        if (j < per && t == 0) {
+            lb[(size_t)qi * per + j] = b;
+            dist[(size_t)qi * per + j] = dd;
+        }
+    }
+}
+
+cudaError_t launch_filter_bounds(const SearchArgs &a, const uint32_t *ids, uint32_t per, float *lb, float *dist,
+                                 cudaStream_t st) {
+    if (a.D.ld > 256) return cudaErrorInvalidValue;
+    const uint32_t grid = (a.nq + 7) / 8;
+    if (a.prec == 1) filter_bounds_kernel<1><<<grid, 256, 0, st>>>(a, ids, per, lb, dist);
+    else if (a.prec == 2) filter_bounds_kernel<2><<<grid, 256, 0, st>>>(a, ids, per, lb, dist);
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
 }
 
 size_t search_warp_smem_bytes(uint32_t ld, uint32_t cap, uint32_t rcap) {
@@ -439,14 +644,20 @@ size_t search_warp_smem_bytes(uint32_t ld, uint32_t cap, uint32_t rcap) {
 namespace {
 
 using SearchFn = void (*)(SearchArgs);
-// The compiled (D-split, prefetch) variants.
-SearchFn search_fn(uint32_t split, uint32_t prefetch) {
-    const bool pf = prefetch > 0;
+template <int PREC>
+SearchFn search_fn_prec(uint32_t split, bool pf) {
     switch (split) {
-        case 2: return pf ? search_kernel<2, 2> : search_kernel<2, 0>;
-        case 8: return pf ? search_kernel<8, 2> : search_kernel<8, 0>;
-        default: return pf ? search_kernel<4, 2> : search_kernel<4, 0>;
+        case 2: return pf ? search_kernel<2, 2, PREC> : search_kernel<2, 0, PREC>;
+        case 8: return pf ? search_kernel<8, 2, PREC> : search_kernel<8, 0, PREC>;
+        default: return pf ? search_kernel<4, 2, PREC> : search_kernel<4, 0, PREC>;
     }
+}
+// The compiled (D-split, prefetch, filter precision) variants.
+SearchFn search_fn(uint32_t split, uint32_t prefetch, uint32_t prec) {
+    const bool pf = prefetch > 0;
+    if (prec == 1) return search_fn_prec<1>(split, pf);
+    if (prec == 2) return search_fn_prec<2>(split, pf);
+    return search_fn_prec<0>(split, pf);
 }
 
 // Warps per block: the requested query tile, or as many as fit 200 KB of
@@ -473,7 +684,7 @@ cudaError_t launch_search(SearchArgs &a, const SearchShape &sh, int num_sms, cud
     if ((size_t)wpb * a.warp_smem_bytes > 227 * 1024) return cudaErrorInvalidValue;
     a.warps_per_block = wpb;
     size_t smem = (size_t)wpb * a.warp_smem_bytes;
-    SearchFn fn = search_fn(sh.split, sh.prefetch);
+    SearchFn fn = search_fn(sh.split, sh.prefetch, a.prec);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
@@ -494,7 +705,7 @@ uint32_t search_max_slots(const SearchArgs &a, const SearchShape &sh, int num_sm
     const size_t wb = search_warp_smem_bytes(a.D.ld, a.cap, a.rcap);
     const uint32_t wpb = pick_wpb(sh, wb);
     const size_t smem = (size_t)wpb * wb;
-    SearchFn fn = search_fn(sh.split, sh.prefetch);
+    SearchFn fn = search_fn(sh.split, sh.prefetch, a.prec);
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, wpb * 32, smem);

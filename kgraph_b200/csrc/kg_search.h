@@ -31,7 +31,11 @@ struct SearchArgs {
     uint32_t vwords, visited_slots;
     uint32_t *qcounter;         // zeroed before launch
     uint32_t *err;              // device error word
-    unsigned long long *work;   // [0] distance evaluations, [1] adjacency entries read (may be null)
+    unsigned long long *work;   // [0] distance evaluations, [1] adjacency entries read, [2] filter
+                                //  evaluations on compressed rows, [3] of those skipped (may be null)
+    uint32_t prec;              // 0 FP32; 1 BF16, 2 FP8 E4M3 compressed rows filter the walk's candidates
+    const void *Xc;             // compressed rows (ld elements each)
+    const float4 *cmeta;        // per row {error bound, scale, norm term, 0}
     uint32_t cap, rcap;         // smem capacities: max(K+P+1), max(K+1)
     uint32_t warps_per_block, warp_smem_bytes;   // filled by launch_search
 };
@@ -49,5 +53,9 @@ size_t search_warp_smem_bytes(uint32_t ld, uint32_t cap, uint32_t rcap);
 // Upper bound of concurrently resident warps (= visited slots needed).
 uint32_t search_max_slots(const SearchArgs &a, const SearchShape &sh, int num_sms);
 cudaError_t launch_search(SearchArgs &a, const SearchShape &sh, int num_sms, cudaStream_t st, uint32_t *grid_out);
+// Filter lower bounds and canonical distances of `per` rows (ids) per query of a.Q
+// (rows of a.q_ld floats, a.D.ld <= 256), with the compressed rows of a.prec.
+cudaError_t launch_filter_bounds(const SearchArgs &a, const uint32_t *ids, uint32_t per, float *lb, float *dist,
+                                 cudaStream_t st);
 
 }  // namespace kgb
