@@ -617,6 +617,25 @@ def main():
                       "speedup_vs_plain": r_value / value, "search_ms_per_step": sum(r_search_ms) / args.steps,
                       "autotune": tune_router,
                       "algorithmic_bytes_per_launch": int(r_evals * (DIM * 4 + 4) + r_adj * 4)}
+            # the same router-seeded walk with the BF16 / FP8 distance filter (results identical)
+            prec = {}
+            for mode in ("bf16", "fp8"):
+                ctx.set_search_precision(mode)
+                for _ in range(args.warmup):
+                    step_router()
+                pm = []
+                for _ in range(args.steps):
+                    flush.fill_(1.0)
+                    torch.cuda.synchronize()
+                    pm.append(step_router()[1])
+                fs = ctx.search_filter_stats()
+                prec[mode] = {"search_ms_per_step": sum(pm) / len(pm),
+                              "value": N_QUERIES / ((sum(pm) / len(pm) + sum(r_ms) / args.steps -
+                                                     sum(r_search_ms) / args.steps) / 1000),
+                              "filter_evaluations": fs["approx"], "fp32_evaluations_skipped": fs["skipped"],
+                              "max_rel_row_error": fs["max_rel_row_error"]}
+            ctx.set_search_precision("fp32")
+            router["distance_filter"] = prec
         else:
             router = {"unavailable": "recall target not reached on the router ladder", "recall_ladder": r_ladder,
                       "train": rinfo}

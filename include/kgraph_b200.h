@@ -115,11 +115,15 @@ int kg_search_batch(kg_ctx *ctx, const float *queries, size_t nq, size_t q_strid
  *                    0 = as many as fit 200 KB of shared memory, at most 8
  *   prefetch         neighbour batches whose rows are prefetched into L2 ahead
  *                    of the walk (0 or 2)
+ *   regs             registers per thread the kernel is compiled for: 64
+ *                    (0 = 64), or 80 (FP32 walk only: fewer spills where
+ *                    large pools limit residency anyway)
  * ms / default_ms / variants are filled by kg_search_autotune. */
 typedef struct {
     unsigned split, warps_per_block, prefetch;
     float ms, default_ms;
     unsigned variants;
+    unsigned regs;
 } kg_search_tuning;
 /* Times every shape on `queries` (a representative sample), checks that all
  * of them return identical ids, distances, counts and costs, and keeps the

@@ -62,7 +62,7 @@ class JoinStats(C.Structure):
 
 class SearchTuning(C.Structure):
     _fields_ = [("split", C.c_uint), ("warps_per_block", C.c_uint), ("prefetch", C.c_uint), ("ms", C.c_float),
-                ("default_ms", C.c_float), ("variants", C.c_uint)]
+                ("default_ms", C.c_float), ("variants", C.c_uint), ("regs", C.c_uint)]
 
 
 class FilterStats(C.Structure):
@@ -314,14 +314,14 @@ class Context:
                                               _ptr(pq), _ptr(ii), 0 if ii is None else ii.shape[1], C.byref(t)))
         return {f: getattr(t, f) for f, _ in SearchTuning._fields_}
 
-    def set_search_tuning(self, split=4, warps_per_block=0, prefetch=2):
-        t = SearchTuning(split, warps_per_block, prefetch, 0.0, 0.0, 0)
+    def set_search_tuning(self, split=4, warps_per_block=0, prefetch=2, regs=64):
+        t = SearchTuning(split, warps_per_block, prefetch, 0.0, 0.0, 0, regs)
         self._check(self.L.kg_set_search_tuning(self.h, C.byref(t)))
 
     def search_tuning(self):
         t = SearchTuning()
         self._check(self.L.kg_get_search_tuning(self.h, C.byref(t)))
-        return {"split": t.split, "warps_per_block": t.warps_per_block, "prefetch": t.prefetch}
+        return {"split": t.split, "warps_per_block": t.warps_per_block, "prefetch": t.prefetch, "regs": t.regs}
 
     def set_search_precision(self, mode):
         """'fp32' (default), 'bf16' or 'fp8': compressed rows that filter the walk's candidates."""

@@ -510,6 +510,7 @@ SearchShape shape_of(const kg_search_tuning &t) {
     sh.split = t.split;
     sh.warps_per_block = t.warps_per_block;
     sh.prefetch = t.prefetch;
+    sh.regs = t.regs;
     return sh;
 }
 }  // namespace
@@ -520,7 +521,7 @@ int kg_set_search_tuning(kg_ctx *ctx, const kg_search_tuning *t) {
     const SearchShape sh = shape_of(*t);
     if (!search_shape_valid(sh) || sh.split == 0)
         return set_error(ctx, KG_E_INVALID, "search tuning: split must be 2, 4 or 8, warps_per_block 0, 1, 2, 4 or "
-                                            "8, prefetch 0 or 2");
+                                            "8, prefetch 0 or 2, regs 0, 64 or 80");
     ctx->search_shape = sh;
     return KG_OK;
 }
@@ -532,6 +533,7 @@ int kg_get_search_tuning(kg_ctx *ctx, kg_search_tuning *t) {
     t->split = ctx->search_shape.split;
     t->warps_per_block = ctx->search_shape.warps_per_block;
     t->prefetch = ctx->search_shape.prefetch;
+    t->regs = ctx->search_shape.regs;
     return KG_OK;
 }
 
@@ -583,11 +585,15 @@ int kg_search_autotune(kg_ctx *ctx, const float *queries, size_t nq, size_t q_st
     ref_ids = ids; ref_d = dists; ref_n = counts; ref_c = costs;
     top_ms = def_ms;
     ++variants;
+    // the 80-register budget only has FP32-walk variants
+    const std::vector<uint32_t> budgets =
+        ctx->search_prec == KG_SEARCH_FP32 ? std::vector<uint32_t>{64u, 80u} : std::vector<uint32_t>{64u};
+    for (uint32_t regs : budgets)
     for (uint32_t split : {2u, 4u, 8u})
         for (uint32_t wpb : {2u, 4u, 8u})
             for (uint32_t pf : {0u, 2u}) {
                 SearchShape sh;
-                sh.split = split; sh.warps_per_block = wpb; sh.prefetch = pf;
+                sh.split = split; sh.warps_per_block = wpb; sh.prefetch = pf; sh.regs = regs;
                 float ms = 0.f;
                 if ((r = run(sh, &ms)) != KG_OK) return r;
                 ++variants;
@@ -605,6 +611,7 @@ int kg_search_autotune(kg_ctx *ctx, const float *queries, size_t nq, size_t q_st
         best->split = top.split;
         best->warps_per_block = top.warps_per_block;
         best->prefetch = top.prefetch;
+        best->regs = top.regs;
         best->ms = top_ms;
         best->default_ms = def_ms;
         best->variants = variants;

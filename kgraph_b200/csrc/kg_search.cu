@@ -130,24 +130,25 @@ __device__ uint32_t warp_bruteforce(const SearchArgs &a, const WarpSmem &s, floa
 
 // Distances of the candidate lanes in `cm` (each holds its id), computed 32/G
 // at a time by the G-lane groups; every candidate lane returns its own distance.
-// Everything stays in registers (no shared-memory staging, so no barrier waits
-// on memory operations still in flight).
+// The candidates' ids are compacted through the warp's 32-entry staging array
+// (rank order), the distances come back by shuffle.
 template <int G>
-__device__ __forceinline__ float warp_cand_dist(const SearchArgs &a, const float *q, float qn, unsigned cm, bool cand,
-                                               uint32_t id, int lane) {
+__device__ __forceinline__ float warp_cand_dist(const SearchArgs &a, const float *q, float qn, uint32_t *stage,
+                                               unsigned cm, bool cand, uint32_t id, int lane) {
     constexpr uint32_t PER = 32 / G;
     const int g = lane / G, t = lane % G;
     const uint32_t n = __popc(cm);
     const uint32_t my = __popc(cm & ((1u << lane) - 1u));
     float mine = 0.f;
+    if (cand) stage[my] = id;
+    __syncwarp();
     for (uint32_t base = 0; base < n; base += PER) {
         const uint32_t i = base + g;
-        const int src = i < n ? (int)__fns(cm, 0, i + 1) : 0;
-        const uint32_t cid = __shfl_sync(FULL, id, src);
-        const float dd = query_dist_g<G>(a.D, q, qn, i < n ? cid : 0u, t, FULL);
+        const float dd = query_dist_g<G>(a.D, q, qn, i < n ? stage[i] : 0u, t, FULL);
         const float got = __shfl_sync(FULL, dd, (int)(G * (my % PER)));
         if (cand && my / PER == base / PER) mine = got;
     }
+    __syncwarp();   // the staging array is reused by the next batch
     return mine;
 }
 
@@ -296,8 +297,11 @@ __device__ __forceinline__ void prefetch_crow(const SearchArgs &a, uint32_t id) 
 // G: lanes per distance (the D-split, 32/G candidates per pass); PF: neighbour
 // batches whose rows are prefetched into L2 ahead of the walk; PREC: 0, or the
 // compressed rows (1 BF16, 2 FP8) that filter candidates once the pool is full.
-template <int G, int PF, int PREC>
-__global__ void __launch_bounds__(256, 4) search_kernel(SearchArgs a) {
+// MB: resident blocks of 256 threads per SM the register allocation is sized
+// for (4: 64 registers per thread; 3: 80, fewer spills for large pools, whose
+// shared memory limits residency anyway).
+template <int G, int PF, int PREC, int MB>
+__global__ void __launch_bounds__(256, MB) search_kernel(SearchArgs a) {
     extern __shared__ __align__(16) char smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -511,7 +515,7 @@ __global__ void __launch_bounds__(256, 4) search_kernel(SearchArgs a) {
                             n_skip += __popc(nm & ~km);
                             if (km) {
                                 const uint32_t aM = keep ? actual_M(a, a.Mp, id) : 0u;
-                                const float dd = warp_cand_dist<G>(a, s.q, qn, km, keep, id, lane);
+                                const float dd = warp_cand_dist<G>(a, s.q, qn, s.cid, km, keep, id, lane);
                                 const unsigned im = __ballot_sync(FULL, keep && dd < worst);
                                 if (im) {
                                     uint32_t mr;
@@ -531,7 +535,7 @@ __global__ void __launch_bounds__(256, 4) search_kernel(SearchArgs a) {
                                 isnew = !(atomicOr(vis + (id >> 5), bit) & bit);
                                 aM = actual_M(a, a.Mp, id);
                             }
-                            const float dd = warp_cand_dist<G>(a, s.q, qn, cm, cand, id, lane);
+                            const float dd = warp_cand_dist<G>(a, s.q, qn, s.cid, cm, cand, id, lane);
                             const unsigned nm = __ballot_sync(FULL, isnew);
                             n_comps += __popc(nm);
                             // A full pool takes a candidate only below its last entry: one at or
@@ -644,20 +648,21 @@ size_t search_warp_smem_bytes(uint32_t ld, uint32_t cap, uint32_t rcap) {
 namespace {
 
 using SearchFn = void (*)(SearchArgs);
-template <int PREC>
+template <int PREC, int MB>
 SearchFn search_fn_prec(uint32_t split, bool pf) {
     switch (split) {
-        case 2: return pf ? search_kernel<2, 2, PREC> : search_kernel<2, 0, PREC>;
-        case 8: return pf ? search_kernel<8, 2, PREC> : search_kernel<8, 0, PREC>;
-        default: return pf ? search_kernel<4, 2, PREC> : search_kernel<4, 0, PREC>;
+        case 2: return pf ? search_kernel<2, 2, PREC, MB> : search_kernel<2, 0, PREC, MB>;
+        case 8: return pf ? search_kernel<8, 2, PREC, MB> : search_kernel<8, 0, PREC, MB>;
+        default: return pf ? search_kernel<4, 2, PREC, MB> : search_kernel<4, 0, PREC, MB>;
     }
 }
-// The compiled (D-split, prefetch, filter precision) variants.
-SearchFn search_fn(uint32_t split, uint32_t prefetch, uint32_t prec) {
+// The compiled (D-split, prefetch, filter precision, register budget) variants;
+// the 80-register budget exists for the FP32 walk.
+SearchFn search_fn(uint32_t split, uint32_t prefetch, uint32_t prec, uint32_t regs) {
     const bool pf = prefetch > 0;
-    if (prec == 1) return search_fn_prec<1>(split, pf);
-    if (prec == 2) return search_fn_prec<2>(split, pf);
-    return search_fn_prec<0>(split, pf);
+    if (prec == 1) return search_fn_prec<1, 4>(split, pf);
+    if (prec == 2) return search_fn_prec<2, 4>(split, pf);
+    return regs == 80 ? search_fn_prec<0, 3>(split, pf) : search_fn_prec<0, 4>(split, pf);
 }
 
 // Warps per block: the requested query tile, or as many as fit 200 KB of
@@ -675,7 +680,8 @@ bool search_shape_valid(const SearchShape &sh) {
     const bool wpb_ok = sh.warps_per_block == 0 || sh.warps_per_block == 1 || sh.warps_per_block == 2 ||
                         sh.warps_per_block == 4 || sh.warps_per_block == 8;
     const bool pf_ok = sh.prefetch == 0 || sh.prefetch == 2;
-    return split_ok && wpb_ok && pf_ok;
+    const bool regs_ok = sh.regs == 0 || sh.regs == 64 || sh.regs == 80;
+    return split_ok && wpb_ok && pf_ok && regs_ok;
 }
 
 cudaError_t launch_search(SearchArgs &a, const SearchShape &sh, int num_sms, cudaStream_t st, uint32_t *grid_out) {
@@ -684,7 +690,7 @@ cudaError_t launch_search(SearchArgs &a, const SearchShape &sh, int num_sms, cud
     if ((size_t)wpb * a.warp_smem_bytes > 227 * 1024) return cudaErrorInvalidValue;
     a.warps_per_block = wpb;
     size_t smem = (size_t)wpb * a.warp_smem_bytes;
-    SearchFn fn = search_fn(sh.split, sh.prefetch, a.prec);
+    SearchFn fn = search_fn(sh.split, sh.prefetch, a.prec, sh.regs);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
@@ -705,7 +711,7 @@ uint32_t search_max_slots(const SearchArgs &a, const SearchShape &sh, int num_sm
     const size_t wb = search_warp_smem_bytes(a.D.ld, a.cap, a.rcap);
     const uint32_t wpb = pick_wpb(sh, wb);
     const size_t smem = (size_t)wpb * wb;
-    SearchFn fn = search_fn(sh.split, sh.prefetch, a.prec);
+    SearchFn fn = search_fn(sh.split, sh.prefetch, a.prec, sh.regs);
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, wpb * 32, smem);

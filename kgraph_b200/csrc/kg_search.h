@@ -42,10 +42,11 @@ struct SearchArgs {
 
 // Launch shape of the search kernel: the D-split (lanes per distance, 2/4/8;
 // 32/split candidates per pass), the query tile (warps = queries per block,
-// 1/2/4/8; 0 = as many as fit, at most 8) and the L2 prefetch depth (0 or 2
-// neighbour batches).  Every shape computes the same bits.
+// 1/2/4/8; 0 = as many as fit, at most 8), the L2 prefetch depth (0 or 2
+// neighbour batches) and the register budget per thread (64, or 80 for the
+// FP32 walk; 0 = 64).  Every shape computes the same bits.
 struct SearchShape {
-    uint32_t split = 4, warps_per_block = 0, prefetch = 2;
+    uint32_t split = 4, warps_per_block = 0, prefetch = 2, regs = 64;
 };
 bool search_shape_valid(const SearchShape &sh);
 

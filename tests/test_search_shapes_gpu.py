@@ -1,7 +1,7 @@
 """Search launch shapes and the autotuner, through the C-ABI.
 
 Every shape of the search kernel -- D-split (lanes per distance), query tile
-(warps per block) and L2 prefetch depth -- must return the reference's
+(warps per block), L2 prefetch depth and register budget -- must return the reference's
 results bit for bit: the reference's fixtures and the oracle on random
 graphs with tails (D % 16 != 0), per-query K/P and T > 1.  The autotuner
 must time every shape, find them all identical and keep the fastest.
@@ -14,7 +14,7 @@ from oracle import kgoracle as ko
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [(s, w, p) for s in (2, 4, 8) for w in (1, 2, 8) for p in (0, 2)]
+SHAPES = [(s, w, p, r) for s in (2, 4, 8) for w in (1, 2, 8) for p in (0, 2) for r in (64, 80)]
 
 
 def bits(a):
@@ -30,13 +30,13 @@ def random_graph(rng, n, dmin, dmax):
     return ko.Graph(off, ids, np.zeros(len(ids), np.float32), M)
 
 
-@pytest.mark.parametrize("split,wpb,pf", SHAPES)
-def test_every_shape_matches_reference_fixture(gpu_ctx, split, wpb, pf):
+@pytest.mark.parametrize("split,wpb,pf,regs", SHAPES)
+def test_every_shape_matches_reference_fixture(gpu_ctx, split, wpb, pf, regs):
     g = load_golden("mix32")
     G = ko.read_index(g["index_bytes"])
     gpu_ctx.set_data(g["X"], g["metric"])
     gpu_ctx.set_graph(G.offsets, G.ids, G.dists, G.M)
-    gpu_ctx.set_search_tuning(split, wpb, pf)
+    gpu_ctx.set_search_tuning(split, wpb, pf, regs)
     try:
         for i, s in enumerate(g["searches"]):
             init_ids = g.get("s%d_init" % i)
@@ -98,8 +98,8 @@ def test_autotune_keeps_fastest_identical_shape(gpu_ctx):
     gpu_ctx.set_graph(G.offsets, G.ids, G.dists, G.M)
     before = gpu_ctx.search(Q, K=10, P=64)
     best = gpu_ctx.search_autotune(Q, K=10, P=64)
-    assert best["variants"] == 19 and best["ms"] <= best["default_ms"]
-    assert gpu_ctx.search_tuning() == {k: best[k] for k in ("split", "warps_per_block", "prefetch")}
+    assert best["variants"] == 37 and best["ms"] <= best["default_ms"]
+    assert gpu_ctx.search_tuning() == {k: best[k] for k in ("split", "warps_per_block", "prefetch", "regs")}
     after = gpu_ctx.search(Q, K=10, P=64)
     for a, b in zip(before, after):
         assert (np.asarray(a).view(np.uint32) == np.asarray(b).view(np.uint32)).all()
