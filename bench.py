@@ -599,15 +599,15 @@ def main():
             torch.cuda.nvtx.range_pop()
             r_value, _ = replica_throughput(sum(r_ms), N_QUERIES, args.steps, dist, world, "cuda")
             r_evals, r_adj = ctx.search_work()
-            # end to end through the C-ABI with host buffers: seeds, then the seeded search
+            # end to end through the C-ABI with host buffers: one kg_router_search call (router seeds and
+            # the seeded walk; queries cross once, seeds stay on the GPU)
             hs = np.zeros((N_QUERIES, 10), np.uint32)
             r_e2e_ms = []
             for it in range(args.warmup + args.steps):
                 torch.cuda.synchronize()
                 t0 = time.perf_counter()
-                ctx.router_seeds_raw(capi._ptr(Qh), N_QUERIES, Qh.strides[0], ROUTER_SEEDS, capi._ptr(hs), 10)
-                ctx.search_raw(capi._ptr(Qh), N_QUERIES, Qh.strides[0], rparams, None, None, 10, capi._ptr(hs),
-                               capi._ptr(hd), capi._ptr(hc), None)
+                ctx.router_search_raw(capi._ptr(Qh), N_QUERIES, Qh.strides[0], rparams, 10, capi._ptr(hs),
+                                      capi._ptr(hd), capi._ptr(hc), None)
                 if it >= args.warmup:
                     r_e2e_ms.append(1000 * (time.perf_counter() - t0))
             r_e2e, _ = replica_throughput(sum(r_e2e_ms), N_QUERIES, args.steps, dist, world, "cuda")
@@ -694,10 +694,13 @@ def main():
                 "build": {"seconds": build_ms / 1000, "wall_s": build_wall, "info": info,
                           "first_build_seconds": cold_ms / 1000, "first_build_wall_s": cold_wall,
                           "graph_launches": build_graphs},
-                "e2e": {"value": head_e2e, "unit": UNIT, "h2d_bytes_per_step": int(Qh.nbytes),
+                # per step: the queries in, and the ids buffer in (the library keeps a caller's entries
+                # beyond each query's result count, as the reference does); ids, distances, counts out
+                "e2e": {"value": head_e2e, "unit": UNIT, "h2d_bytes_per_step": int(Qh.nbytes + hi.nbytes),
                         "d2h_bytes_per_step": int(hi.nbytes + hd.nbytes + hc.nbytes)},
-                # router path per step: 5 kernels per 4096-query chunk (features, 3 GEMMs, top-m) + the search
-                "gpu_launches": args.steps * (1 + 5 * ((N_QUERIES + 4095) // 4096)) if best_router else args.steps,
+                # router path per step: 6 kernels per 4096-query chunk (features, 3 GEMMs, top clusters,
+                # seed ranking) + the search
+                "gpu_launches": args.steps * (1 + 6 * ((N_QUERIES + 4095) // 4096)) if best_router else args.steps,
                 "roofline": ({"bound": "hbm", "kernel": "search_kernel (router-seeded)",
                               "achieved": router["roofline"]["achieved"], "peak": hbm, "unit": "GB/s",
                               "frac": router["roofline"]["frac"], "traffic": None,

@@ -233,6 +233,13 @@ int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const float *train_q
  * out_ld); pass them to kg_search_batch as ids with params->init = m (m < K). */
 int kg_router_seeds(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes, unsigned m, uint32_t *seeds,
                     size_t out_ld);
+/* kg_router_seeds followed by kg_search_batch in one call: the queries cross
+ * to the GPU once and the seeds never leave it.  params->init is the number of
+ * router seeds per query (0 < init < K); ids is output only.  Results equal
+ * kg_router_seeds + kg_search_batch(init) on the same queries. */
+int kg_router_search(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes,
+                     const kg_search_params *params, size_t out_ld, uint32_t *ids, float *dists, uint32_t *counts,
+                     float *costs);
 /* Mean loss and gradients (W1|b1|W2|b2|W3|b3, FP32, row-major in x out) of the
  * MLP on n <= 4096 labelled rows, with `weights` (same layout, may be NULL to
  * keep the current ones) and identity input normalisation: the check of the

@@ -23,7 +23,7 @@ SYMBOLS = [
     "kg_router_params_default", "kg_router_train", "kg_router_seeds", "kg_router_gradients", "kg_last_router_timing",
     "kg_set_join_precision", "kg_last_join_stats", "kg_last_build_graphs", "kg_search_autotune",
     "kg_set_search_tuning", "kg_get_search_tuning", "kg_set_search_precision", "kg_last_search_filter",
-    "kg_filter_bounds",
+    "kg_filter_bounds", "kg_router_search",
 ]
 
 JOIN = {"auto": 0, "fp32": 1, "bf16": 2, "bf16_always": 3}
@@ -123,6 +123,7 @@ def lib():
         L.kg_set_search_precision.argtypes = [vp, C.c_int]
         L.kg_last_search_filter.argtypes = [vp, C.POINTER(FilterStats)]
         L.kg_filter_bounds.argtypes = [vp, vp, sz, sz, vp, sz, vp, vp]
+        L.kg_router_search.argtypes = [vp, vp, sz, sz, C.POINTER(SearchParams), sz, vp, vp, vp, vp]
         L.kg_index_params_default.argtypes = [C.POINTER(IndexParams)]
         L.kg_search_params_default.argtypes = [C.POINTER(SearchParams)]
         _lib = L
@@ -255,6 +256,25 @@ class Context:
         seeds = np.zeros((Q.shape[0], ld), np.uint32)
         self._check(self.L.kg_router_seeds(self.h, _ptr(Q), Q.shape[0], Q.strides[0], m, _ptr(seeds), ld))
         return seeds
+
+    def router_search(self, Q, K=10, P=10, seeds=3, S=10, epsilon=1e30, out_ld=None, with_cost=True):
+        """Router seeds + seeded walk in one call; returns (ids, dists, counts, costs)."""
+        Q = np.ascontiguousarray(Q, np.float32)
+        nq = Q.shape[0]
+        ld = out_ld or K
+        p = SearchParams(K, 0, P, S, 1, epsilon, 1998, seeds)
+        ids = np.zeros((nq, ld), np.uint32)
+        dists = np.zeros((nq, ld), np.float32)
+        counts = np.zeros(nq, np.uint32)
+        costs = np.zeros(nq, np.float32) if with_cost else None
+        self._check(self.L.kg_router_search(self.h, _ptr(Q), nq, Q.strides[0], C.byref(p), ld, _ptr(ids), _ptr(dists),
+                                            _ptr(counts), _ptr(costs)))
+        return ids, dists, counts, costs
+
+    def router_search_raw(self, q_ptr, nq, q_stride, params, out_ld, ids_ptr, d_ptr, c_ptr, cost_ptr):
+        """kg_router_search on raw (device or host) pointers."""
+        self._check(self.L.kg_router_search(self.h, q_ptr, nq, q_stride, C.byref(params), out_ld, ids_ptr, d_ptr,
+                                            c_ptr, cost_ptr))
 
     def router_seeds_raw(self, q_ptr, nq, q_stride, m, seeds_ptr, out_ld):
         """kg_router_seeds on raw (device or host) pointers; returns its device milliseconds."""

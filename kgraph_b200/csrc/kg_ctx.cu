@@ -157,6 +157,7 @@ void kg_ctx_destroy(kg_ctx *c) {
                       &c->out_ids, &c->out_d, &c->out_cnt, &c->out_cost, &c->tcstat, &c->joinq, &c->joinaux, &c->joinb};
     for (DevBuf *b : bufs) b->release();
     for (auto &b : c->build_scratch) b.release();
+    c->rseeds.release();
     kgb::router_release(c->router);
     cudaEventDestroy(c->ev0);
     cudaEventDestroy(c->ev1);
@@ -298,12 +299,15 @@ int ensure_search_layout(kg_ctx *ctx) {
 
 }  // extern "C"
 
-namespace {
+namespace kgb {
 
-// kg_search_batch with the context lock held, in launch shape `sh`.
+// kg_search_batch with the context lock held, in launch shape `sh`.  With
+// init_dev (device rows of init_ld ids) the starting points come from there
+// instead of from `ids`.
 int search_locked(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes,
                   const kg_search_params *params, const uint32_t *K_per_q, const uint32_t *P_per_q, size_t out_ld,
-                  uint32_t *ids, float *dists, uint32_t *counts, float *costs, const SearchShape &sh) {
+                  uint32_t *ids, float *dists, uint32_t *counts, float *costs, const SearchShape &sh,
+                  const uint32_t *init_dev, size_t init_ld) {
     if (!ctx->has_data) return set_error(ctx, KG_E_RUNTIME, "no dataset");
     if (!params || !ids || !counts) return set_error(ctx, KG_E_INVALID, "bad arguments");
     if (nq == 0) return KG_OK;
@@ -434,7 +438,11 @@ int search_locked(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_
     } else a.out_ids = ids;
     if (a.init) {
         if ((e = ctx->init_ids.reserve(Q * out_ld * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc init");
-        cudaMemcpyAsync(ctx->init_ids.p, ids, Q * out_ld * 4, cudaMemcpyDefault, ctx->stream);
+        if (init_dev)
+            cudaMemcpy2DAsync(ctx->init_ids.p, out_ld * 4, init_dev, init_ld * 4, (size_t)a.init * 4, Q,
+                              cudaMemcpyDeviceToDevice, ctx->stream);
+        else
+            cudaMemcpyAsync(ctx->init_ids.p, ids, Q * out_ld * 4, cudaMemcpyDefault, ctx->stream);
         a.init_ids = ctx->init_ids.as<uint32_t>();
     }
     if (!ids_dev) {   // keep caller's untouched tail entries (the reference leaves them as they were)
@@ -491,7 +499,7 @@ int search_locked(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_
     return check_device_error(ctx, "search");
 }
 
-}  // namespace
+}  // namespace kgb
 
 extern "C" {
 
@@ -501,7 +509,7 @@ int kg_search_batch(kg_ctx *ctx, const float *queries, size_t nq, size_t q_strid
     if (!ctx) return KG_E_INVALID;
     Lock lk(ctx);
     return search_locked(ctx, queries, nq, q_stride_bytes, params, K_per_q, P_per_q, out_ld, ids, dists, counts,
-                         costs, ctx->search_shape);
+                         costs, ctx->search_shape, nullptr, 0);
 }
 
 namespace {
@@ -572,7 +580,7 @@ int kg_search_autotune(kg_ctx *ctx, const float *queries, size_t nq, size_t q_st
         for (int rep = 0; rep < 3; ++rep) {   // one warm-up, the faster of two timed runs
             if (params->init) ids = init_rows;
             int r = search_locked(ctx, queries, nq, q_stride_bytes, params, K_per_q, P_per_q, ld, ids.data(),
-                                  dists.data(), counts.data(), costs.data(), sh);
+                                  dists.data(), counts.data(), costs.data(), sh, nullptr, 0);
             if (r != KG_OK) return r;
             if (rep > 0) bestv = std::min(bestv, ctx->last_search_ms);
         }

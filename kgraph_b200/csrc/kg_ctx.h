@@ -88,6 +88,7 @@ struct kg_ctx {
     kgb::DevBuf joinq, joinaux, joinb;   // tensor-core join: candidate queue, worst-case prefix, round bounds
     kg_join_stats last_join{};
     kgb::RouterState *router = nullptr;   // learned entry router (kg_router.cu)
+    kgb::DevBuf rseeds;                   // router seeds handed to the search (kg_router_search)
 };
 
 namespace kgb {
@@ -98,6 +99,12 @@ int cuda_fail(kg_ctx *ctx, cudaError_t e, const char *what);
 bool is_device_ptr(const void *p);
 // Reads and clears the device error word; returns KG_OK or sets the message.
 int check_device_error(kg_ctx *ctx, const char *what);
+// kg_search_batch with the context lock held (kg_ctx.cu); init_dev, when not
+// null, holds the starting points (device rows of init_ld ids).
+int search_locked(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes,
+                  const kg_search_params *params, const uint32_t *K_per_q, const uint32_t *P_per_q, size_t out_ld,
+                  uint32_t *ids, float *dists, uint32_t *counts, float *costs, const SearchShape &sh,
+                  const uint32_t *init_dev, size_t init_ld);
 // Builds the compressed rows of ctx->search_prec if the dataset changed since.
 int ensure_search_precision(kg_ctx *ctx);
 // Exact top-K brute force of `nq` dataset rows (LinearSearch, kgraph.cpp:212-229)

@@ -896,10 +896,10 @@ extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const flo
     return check_device_error(ctx, "router");
 }
 
-extern "C" int kg_router_seeds(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes, unsigned m,
-                               uint32_t *seeds, size_t out_ld) {
-    if (!ctx) return KG_E_INVALID;
-    Guard g(ctx);
+namespace {
+// kg_router_seeds with the context lock held.
+int router_seeds_locked(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes, unsigned m,
+                        uint32_t *seeds, size_t out_ld) {
     if (!ctx->router || !ctx->router->trained) return set_error(ctx, KG_E_RUNTIME, "router not trained");
     RouterState &r = *ctx->router;
     if (m == 0 || m > r.C || m > out_ld || m > 64) return set_error(ctx, KG_E_INVALID, "bad number of router seeds");
@@ -940,6 +940,47 @@ extern "C" int kg_router_seeds(kg_ctx *ctx, const float *queries, size_t nq, siz
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "router seeds");
     cudaEventElapsedTime(&ctx->last_router_ms, ctx->ev0, ctx->ev1);
     return KG_OK;
+}
+}  // namespace
+
+extern "C" int kg_router_seeds(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes, unsigned m,
+                               uint32_t *seeds, size_t out_ld) {
+    if (!ctx) return KG_E_INVALID;
+    Guard g(ctx);
+    return router_seeds_locked(ctx, queries, nq, q_stride_bytes, m, seeds, out_ld);
+}
+
+extern "C" int kg_router_search(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes,
+                                const kg_search_params *params, size_t out_ld, uint32_t *ids, float *dists,
+                                uint32_t *counts, float *costs) {
+    if (!ctx) return KG_E_INVALID;
+    Guard g(ctx);
+    if (!params || !queries || !ids || !counts) return set_error(ctx, KG_E_INVALID, "bad arguments");
+    if (nq == 0) return KG_OK;
+    if (!ctx->router || !ctx->router->trained) return set_error(ctx, KG_E_RUNTIME, "router not trained");
+    if (!ctx->has_graph) return set_error(ctx, KG_E_RUNTIME, "no index");
+    if (params->init == 0 || !(params->init < params->K)) return set_error(ctx, KG_E_INVALID, "L < params.K");
+    if (params->init > out_ld) return set_error(ctx, KG_E_INVALID, "init larger than out_ld");
+    if (q_stride_bytes < ctx->d * sizeof(float)) return set_error(ctx, KG_E_INVALID, "bad query array");
+    cudaStream_t st = ctx->stream;
+    cudaError_t e;
+    // queries once into device rows of the padded width, used by both stages in place
+    const size_t ld = ctx->ld;
+    if ((e = ctx->qbuf.reserve(nq * ld * 4)) != cudaSuccess || (e = ctx->rseeds.reserve(nq * params->init * 4)) !=
+                                                                   cudaSuccess)
+        return cuda_fail(ctx, e, "alloc queries");
+    if (ld != ctx->d) cudaMemsetAsync(ctx->qbuf.p, 0, nq * ld * 4, st);
+    e = cudaMemcpy2DAsync(ctx->qbuf.p, ld * 4, queries, q_stride_bytes, ctx->d * 4, nq,
+                          is_device_ptr(queries) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "copy queries");
+    int rc = router_seeds_locked(ctx, ctx->qbuf.as<float>(), nq, ld * 4, params->init, ctx->rseeds.as<uint32_t>(),
+                                 params->init);
+    if (rc != KG_OK) return rc;
+    const float router_ms = ctx->last_router_ms;
+    rc = search_locked(ctx, ctx->qbuf.as<float>(), nq, ld * 4, params, nullptr, nullptr, out_ld, ids, dists, counts,
+                       costs, ctx->search_shape, ctx->rseeds.as<uint32_t>(), params->init);
+    ctx->last_router_ms = router_ms;
+    return rc;
 }
 
 // Loss and gradients of the current weights on n labelled rows (n <= 4096), for

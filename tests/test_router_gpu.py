@@ -61,4 +61,14 @@ def test_router_beats_plain_seeding_at_equal_P():
     routed, _, cnt, _ = ctx.search(Q, K=10, P=P, init=3, init_ids=seeds)
     r_plain, r_router = recall(plain), recall(routed)
     assert r_router > r_plain and r_router >= 0.9, (r_plain, r_router)
+    # the fused call: same seeds, same walk, same results
+    fi, fd, fc, fk = ctx.router_search(Q, K=10, P=P, seeds=3)
+    _, rd, _, rk = ctx.search(Q, K=10, P=P, init=3, init_ids=seeds)
+    assert (fc == cnt).all() and (fk.view(np.uint32) == rk.view(np.uint32)).all()
+    for q in range(len(Q)):
+        c = int(cnt[q])
+        assert (fi[q, :c] == routed[q, :c]).all()
+        assert (fd[q, :c].view(np.uint32) == rd[q, :c].view(np.uint32)).all()
+    with pytest.raises(capi.KGError, match="L < params.K"):
+        ctx.router_search(Q, K=3, P=P, seeds=3)
     ctx.close()
