@@ -45,9 +45,11 @@ ROUTER_P_LADDER = [10, 20, 30, 50, 100, 200, 300, 500, 1000]
 ROUTER_SEEDS = 3          # starting points per query (the reference requires init < K)
 ROUTER_TRAIN = 200_000    # (query, best node) training pairs
 TARGET = 0.95
-# DRAM read + write of one search launch (10,000 queries, K=10, P=1000) from an
-# ncu capture of the same kernel on the 400k-node version of this workload.
+# DRAM read + write of one search launch (10,000 queries, K=10) from ncu
+# captures of the same kernels on the 400k-node version of this workload:
+# the plain walk at P=1000 and the router-seeded walk at P=10.
 SEARCH_DRAM_BYTES_PER_LAUNCH = 22.09e9
+ROUTER_SEARCH_DRAM_BYTES_PER_LAUNCH = 9.081e9
 
 
 def _sample(c, n, rng, d):
@@ -703,7 +705,7 @@ def main():
                 "gpu_launches": args.steps * (1 + 6 * ((N_QUERIES + 4095) // 4096)) if best_router else args.steps,
                 "roofline": ({"bound": "hbm", "kernel": "search_kernel (router-seeded)",
                               "achieved": router["roofline"]["achieved"], "peak": hbm, "unit": "GB/s",
-                              "frac": router["roofline"]["frac"], "traffic": None,
+                              "frac": router["roofline"]["frac"], "traffic": ROUTER_SEARCH_DRAM_BYTES_PER_LAUNCH,
                               "algorithmic_bytes_per_launch": router["algorithmic_bytes_per_launch"]} if best_router else
                              {"bound": "hbm", "kernel": "search_kernel", "achieved": achieved, "peak": hbm,
                               "unit": "GB/s", "frac": achieved / hbm, "traffic": SEARCH_DRAM_BYTES_PER_LAUNCH,
