@@ -1,0 +1,17 @@
+// Tensor-core GEMM for the router (kg_gemm.cu).
+#pragma once
+#include <cstdint>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+namespace kgb {
+
+// C[M,N] = op(A)[M,K] * op(B)[K,N] (+ beta * C) (+ bias[N]) (ReLU) on tcgen05:
+// BF16 operands, FP32 accumulation in TMEM, FP32 C and optional BF16 copy Cb
+// (same ldc).  ta / tb: A / B stored transposed (K x M / N x K row-major).  A
+// tensor-core wait that runs out sets ERR_TC_TIMEOUT in *err.
+void tc_gemm(cudaStream_t st, int M, int N, int K, const __nv_bfloat16 *A, int lda, int ta, const __nv_bfloat16 *B,
+             int ldb, int tb, float *C, int ldc, __nv_bfloat16 *Cb, const float *bias, int relu, float beta,
+             uint32_t *err);
+
+}  // namespace kgb

@@ -33,70 +33,12 @@
 #include <random>
 #include <vector>
 #include "kg_ctx.h"
+#include "kg_gemm.h"
 #include "kg_warp.cuh"
 
 namespace kgb {
 
 namespace {
-
-constexpr int GT = 64;        // GEMM tile (rows and columns of C per block)
-constexpr int GK = 32;        // K step
-
-// C[M,N] = op(A)[M,K] * op(B)[K,N] (+ bias[N]) (ReLU), FP32 out, optional BF16
-// copy.  op(A) = A (row-major, lda) or A^T (A is K x M, lda); same for B.
-// 256 threads, each 4x4 outputs of a 64x64 tile, operands staged through
-// shared memory as FP32.
-__global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int K, const __nv_bfloat16 *A, int lda, int ta,
-                                                   const __nv_bfloat16 *B, int ldb, int tb, float *C, int ldc,
-                                                   __nv_bfloat16 *Cb, const float *bias, int relu, float beta) {
-    __shared__ float As[GK][GT + 4];
-    __shared__ float Bs[GK][GT + 4];
-    const int tid = threadIdx.x;
-    const int r0 = blockIdx.y * GT, c0 = blockIdx.x * GT;
-    const int tr = (tid / 16) * 4, tc = (tid % 16) * 4;
-    float acc[4][4] = {};
-    for (int k0 = 0; k0 < K; k0 += GK) {
-        for (int e = tid; e < GK * GT; e += 256) {
-            const int kk = e / GT, mm = e % GT;
-            const int r = r0 + mm, k = k0 + kk;
-            float v = 0.f;
-            if (r < M && k < K) v = __bfloat162float(ta ? A[(size_t)k * lda + r] : A[(size_t)r * lda + k]);
-            As[kk][mm] = v;
-            const int c = c0 + mm;
-            float w = 0.f;
-            if (c < N && k < K) w = __bfloat162float(tb ? B[(size_t)c * ldb + k] : B[(size_t)k * ldb + c]);
-            Bs[kk][mm] = w;
-        }
-        __syncthreads();
-#pragma unroll 8
-        for (int kk = 0; kk < GK; ++kk) {
-            float a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) { a[i] = As[kk][tr + i]; b[i] = Bs[kk][tc + i]; }
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = __fmaf_rn(a[i], b[j], acc[i][j]);
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const int r = r0 + tr + i;
-        if (r >= M) continue;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int c = c0 + tc + j;
-            if (c >= N) continue;
-            float v = acc[i][j];
-            if (beta != 0.f) v += beta * C[(size_t)r * ldc + c];
-            if (bias) v += bias[c];
-            if (relu) v = fmaxf(v, 0.f);
-            C[(size_t)r * ldc + c] = v;
-            if (Cb) Cb[(size_t)r * ldc + c] = __float2bfloat16_rn(v);
-        }
-    }
-}
 
 __global__ void to_bf16_kernel(const float *x, __nv_bfloat16 *y, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
@@ -348,10 +290,11 @@ __global__ void __launch_bounds__(RANK_WARPS * 32) seed_rank_kernel(DataView D, 
     }
 }
 
-void gemm(cudaStream_t st, int M, int N, int K, const __nv_bfloat16 *A, int lda, int ta, const __nv_bfloat16 *B,
-          int ldb, int tb, float *C, int ldc, __nv_bfloat16 *Cb, const float *bias, int relu, float beta = 0.f) {
-    dim3 grid((N + GT - 1) / GT, (M + GT - 1) / GT);
-    gemm_kernel<<<grid, 256, 0, st>>>(M, N, K, A, lda, ta, B, ldb, tb, C, ldc, Cb, bias, relu, beta);
+// Every product of the router runs on the tensor cores (kg_gemm.cu).
+void gemm(cudaStream_t st, uint32_t *err, int M, int N, int K, const __nv_bfloat16 *A, int lda, int ta,
+          const __nv_bfloat16 *B, int ldb, int tb, float *C, int ldc, __nv_bfloat16 *Cb, const float *bias, int relu,
+          float beta = 0.f) {
+    tc_gemm(st, M, N, K, A, lda, ta, B, ldb, tb, C, ldc, Cb, bias, relu, beta, err);
 }
 
 int blocks_for(size_t n, int per = 256) { return (int)std::min<size_t>((n + per - 1) / per, 148 * 32); }
@@ -362,6 +305,7 @@ int blocks_for(size_t n, int per = 256) { return (int)std::min<size_t>((n + per 
 // Router state (device): weights, Adam moments, activations for one batch.
 struct RouterState {
     uint32_t D = 0, H = 0, C = 0, batch = 0, probe = 1;
+    uint32_t *err = nullptr;                     // the context's device error word
     uint32_t entries_total = 0, component_entries = 0;   // entry nodes; of which added for uncovered components
     bool trained = false;
     DevBuf mean, inv_std;                        // normalisation
@@ -412,11 +356,11 @@ cudaError_t alloc_router(RouterState &r, uint32_t batch) {
 
 // Forward of B rows already in r.X (BF16 features): H1, H2, Z.
 void forward(cudaStream_t st, RouterState &r, int B) {
-    gemm(st, B, r.H, r.D, r.X.as<__nv_bfloat16>(), r.D, 0, r.wb[0].as<__nv_bfloat16>(), r.H, 0, r.H1.as<float>(), r.H,
+    gemm(st, r.err, B, r.H, r.D, r.X.as<__nv_bfloat16>(), r.D, 0, r.wb[0].as<__nv_bfloat16>(), r.H, 0, r.H1.as<float>(), r.H,
          r.H1b.as<__nv_bfloat16>(), r.b[0].as<float>(), 1);
-    gemm(st, B, r.H, r.H, r.H1b.as<__nv_bfloat16>(), r.H, 0, r.wb[1].as<__nv_bfloat16>(), r.H, 0, r.H2.as<float>(), r.H,
+    gemm(st, r.err, B, r.H, r.H, r.H1b.as<__nv_bfloat16>(), r.H, 0, r.wb[1].as<__nv_bfloat16>(), r.H, 0, r.H2.as<float>(), r.H,
          r.H2b.as<__nv_bfloat16>(), r.b[1].as<float>(), 1);
-    gemm(st, B, r.C, r.H, r.H2b.as<__nv_bfloat16>(), r.H, 0, r.wb[2].as<__nv_bfloat16>(), r.C, 0, r.Z.as<float>(), r.C,
+    gemm(st, r.err, B, r.C, r.H, r.H2b.as<__nv_bfloat16>(), r.H, 0, r.wb[2].as<__nv_bfloat16>(), r.C, 0, r.Z.as<float>(), r.C,
          nullptr, r.b[2].as<float>(), 0);
 }
 
@@ -427,24 +371,24 @@ void backward(cudaStream_t st, RouterState &r, int B) {
     softmax_ce_kernel<<<(B * 32 + 255) / 256, 256, 0, st>>>(r.Z.as<float>(), r.lab.as<int32_t>(), B, r.C,
                                                             r.dZ.as<float>(), r.dZb.as<__nv_bfloat16>(), loss, hits);
     // layer 3: dW3 = H2^T dZ, db3, dH2 = dZ W3^T
-    gemm(st, r.H, r.C, B, r.H2b.as<__nv_bfloat16>(), r.H, 1, r.dZb.as<__nv_bfloat16>(), r.C, 0, r.gw[2].as<float>(), r.C,
+    gemm(st, r.err, r.H, r.C, B, r.H2b.as<__nv_bfloat16>(), r.H, 1, r.dZb.as<__nv_bfloat16>(), r.C, 0, r.gw[2].as<float>(), r.C,
          nullptr, nullptr, 0);
     colsum_kernel<<<(r.C + 255) / 256, 256, 0, st>>>(r.dZ.as<float>(), B, r.C, r.gb[2].as<float>());
-    gemm(st, B, r.H, r.C, r.dZb.as<__nv_bfloat16>(), r.C, 0, r.wb[2].as<__nv_bfloat16>(), r.C, 1, r.dH.as<float>(), r.H,
+    gemm(st, r.err, B, r.H, r.C, r.dZb.as<__nv_bfloat16>(), r.C, 0, r.wb[2].as<__nv_bfloat16>(), r.C, 1, r.dH.as<float>(), r.H,
          nullptr, nullptr, 0);
     relu_grad_kernel<<<blocks_for((size_t)B * r.H), 256, 0, st>>>(r.dH.as<float>(), r.H2.as<float>(),
                                                                   r.dHb.as<__nv_bfloat16>(), (size_t)B * r.H);
     // layer 2
-    gemm(st, r.H, r.H, B, r.H1b.as<__nv_bfloat16>(), r.H, 1, r.dHb.as<__nv_bfloat16>(), r.H, 0, r.gw[1].as<float>(), r.H,
+    gemm(st, r.err, r.H, r.H, B, r.H1b.as<__nv_bfloat16>(), r.H, 1, r.dHb.as<__nv_bfloat16>(), r.H, 0, r.gw[1].as<float>(), r.H,
          nullptr, nullptr, 0);
     colsum_kernel<<<(r.H + 255) / 256, 256, 0, st>>>(r.dH.as<float>(), B, r.H, r.gb[1].as<float>());
     // dH1 = dH2 W2^T (into r.dZ as scratch: B x H fits), then the ReLU mask
-    gemm(st, B, r.H, r.H, r.dHb.as<__nv_bfloat16>(), r.H, 0, r.wb[1].as<__nv_bfloat16>(), r.H, 1, r.dZ.as<float>(), r.H,
+    gemm(st, r.err, B, r.H, r.H, r.dHb.as<__nv_bfloat16>(), r.H, 0, r.wb[1].as<__nv_bfloat16>(), r.H, 1, r.dZ.as<float>(), r.H,
          nullptr, nullptr, 0);
     relu_grad_kernel<<<blocks_for((size_t)B * r.H), 256, 0, st>>>(r.dZ.as<float>(), r.H1.as<float>(),
                                                                   r.dHb.as<__nv_bfloat16>(), (size_t)B * r.H);
     // layer 1
-    gemm(st, r.D, r.H, B, r.X.as<__nv_bfloat16>(), r.D, 1, r.dHb.as<__nv_bfloat16>(), r.H, 0, r.gw[0].as<float>(), r.H,
+    gemm(st, r.err, r.D, r.H, B, r.X.as<__nv_bfloat16>(), r.D, 1, r.dHb.as<__nv_bfloat16>(), r.H, 0, r.gw[0].as<float>(), r.H,
          nullptr, nullptr, 0);
     colsum_kernel<<<(r.H + 255) / 256, 256, 0, st>>>(r.dZ.as<float>(), B, r.H, r.gb[0].as<float>());
 }
@@ -491,9 +435,9 @@ struct KMeansBufs {
 // `seed_rows`: `iters` updates, then a final assignment into lab[n] / best[n]
 // (|c|^2 - 2 f.c of the chosen centroid).  The BF16 centroids end in
 // *centb_out (inside kb.work); `block` holds one block of F.C^T.
-cudaError_t kmeans_run(cudaStream_t st, const __nv_bfloat16 *F, uint32_t n, uint32_t D, uint32_t C, uint32_t iters,
-                       const std::vector<uint32_t> &seed_rows, KMeansBufs &kb, DevBuf &block, int32_t *lab,
-                       float *best, __nv_bfloat16 **centb_out) {
+cudaError_t kmeans_run(cudaStream_t st, uint32_t *err, const __nv_bfloat16 *F, uint32_t n, uint32_t D, uint32_t C,
+                       uint32_t iters, const std::vector<uint32_t> &seed_rows, KMeansBufs &kb, DevBuf &block,
+                       int32_t *lab, float *best, __nv_bfloat16 **centb_out) {
     cudaError_t e;
     const uint32_t brows = (uint32_t)std::max<size_t>(1024, std::min<size_t>(65536, ((size_t)1 << 29) / C));
     if ((e = kb.work.reserve((size_t)C * D * 4 * 2 + (size_t)C * D * 2 + (size_t)C * 8 + 64)) != cudaSuccess ||
@@ -511,7 +455,7 @@ cudaError_t kmeans_run(cudaStream_t st, const __nv_bfloat16 *F, uint32_t n, uint
     for (uint32_t it = 0; it <= iters; ++it) {
         for (uint32_t r0 = 0; r0 < n; r0 += brows) {
             const uint32_t rows = std::min<uint32_t>(brows, n - r0);
-            gemm(st, rows, C, D, F + (size_t)r0 * D, D, 0, centb, D, 1, block.as<float>(), C, nullptr, nullptr, 0);
+            gemm(st, err, rows, C, D, F + (size_t)r0 * D, D, 0, centb, D, 1, block.as<float>(), C, nullptr, nullptr, 0);
             argmin_kernel<<<(rows * 32 + 255) / 256, 256, 0, st>>>(block.as<float>(), cn, rows, C, lab + r0, best + r0);
         }
         if (it == iters) break;
@@ -657,6 +601,7 @@ extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const flo
     cudaError_t e;
     if (!ctx->router) ctx->router = new RouterState;
     RouterState &r = *ctx->router;
+    r.err = ctx->errw.as<uint32_t>();
     r.trained = false;
     r.D = ctx->d;
     r.H = p->hidden;
@@ -699,7 +644,7 @@ extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const flo
     {
         std::vector<uint32_t> pick(Cf);
         for (uint32_t c = 0; c < Cf; ++c) pick[c] = krng() % N;
-        if ((e = kmeans_run(st, F, N, D, Cf, p->kmeans_iters, pick, fine, s3, lab, best, &centf)) != cudaSuccess)
+        if ((e = kmeans_run(st, r.err, F, N, D, Cf, p->kmeans_iters, pick, fine, s3, lab, best, &centf)) != cudaSuccess)
             return cuda_fail(ctx, e, "router kmeans");
     }
     unsigned long long *key = reinterpret_cast<unsigned long long *>(s1.p);
@@ -711,7 +656,7 @@ extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const flo
     if (E > 1) {
         std::vector<uint32_t> pick(C);
         for (uint32_t c = 0; c < C; ++c) pick[c] = krng() % Cf;
-        if ((e = kmeans_run(st, centf, Cf, D, C, p->kmeans_iters, pick, coarse, s3, labc, bestc, &centc)) !=
+        if ((e = kmeans_run(st, r.err, centf, Cf, D, C, p->kmeans_iters, pick, coarse, s3, labc, bestc, &centc)) !=
             cudaSuccess)
             return cuda_fail(ctx, e, "router kmeans");
     }
@@ -902,6 +847,7 @@ int router_seeds_locked(kg_ctx *ctx, const float *queries, size_t nq, size_t q_s
                         uint32_t *seeds, size_t out_ld) {
     if (!ctx->router || !ctx->router->trained) return set_error(ctx, KG_E_RUNTIME, "router not trained");
     RouterState &r = *ctx->router;
+    r.err = ctx->errw.as<uint32_t>();
     if (m == 0 || m > r.C || m > out_ld || m > 64) return set_error(ctx, KG_E_INVALID, "bad number of router seeds");
     cudaStream_t st = ctx->stream;
     cudaError_t e;
@@ -993,6 +939,7 @@ extern "C" int kg_router_gradients(kg_ctx *ctx, unsigned d, unsigned hidden, uns
     if (n == 0 || n > 4096) return set_error(ctx, KG_E_INVALID, "n must be in 1..4096");
     if (!ctx->router) ctx->router = new RouterState;
     RouterState &r = *ctx->router;
+    r.err = ctx->errw.as<uint32_t>();
     cudaStream_t st = ctx->stream;
     cudaError_t e;
     if (weights || r.D != d || r.H != hidden || r.C != clusters) {
