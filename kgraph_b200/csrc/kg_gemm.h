@@ -14,4 +14,11 @@ void tc_gemm(cudaStream_t st, int M, int N, int K, const __nv_bfloat16 *A, int l
              int ldb, int tb, float *C, int ldc, __nv_bfloat16 *Cb, const float *bias, int relu, float beta,
              uint32_t *err);
 
+// k-means assignment on tcgen05: lab[r] = argmin_c cn[c] - 2 F[r].cent[c]
+// (ties: smaller c), best[r] that value; F is n x D, cent C x D (BF16,
+// row-major), D <= 256.  false when the shape is not supported (the caller then
+// uses tc_gemm and a separate argmin).
+bool tc_assign(cudaStream_t st, int n, int D, const __nv_bfloat16 *F, const __nv_bfloat16 *cent, int C, const float *cn,
+               int32_t *lab, float *best, uint32_t *err);
+
 }  // namespace kgb

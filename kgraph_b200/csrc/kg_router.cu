@@ -441,8 +441,9 @@ cudaError_t kmeans_run(cudaStream_t st, uint32_t *err, const __nv_bfloat16 *F, u
     cudaError_t e;
     const uint32_t brows = (uint32_t)std::max<size_t>(1024, std::min<size_t>(65536, ((size_t)1 << 29) / C));
     if ((e = kb.work.reserve((size_t)C * D * 4 * 2 + (size_t)C * D * 2 + (size_t)C * 8 + 64)) != cudaSuccess ||
-        (e = kb.rows.reserve((size_t)C * 4)) != cudaSuccess || (e = block.reserve((size_t)brows * C * 4)) != cudaSuccess)
+        (e = kb.rows.reserve((size_t)C * 4)) != cudaSuccess)
         return e;
+    if (D > 256 && (e = block.reserve((size_t)brows * C * 4)) != cudaSuccess) return e;   // product + argmin path
     float *cent = kb.work.as<float>();
     float *csum = cent + (size_t)C * D;
     __nv_bfloat16 *centb = reinterpret_cast<__nv_bfloat16 *>(csum + (size_t)C * D);
@@ -453,10 +454,15 @@ cudaError_t kmeans_run(cudaStream_t st, uint32_t *err, const __nv_bfloat16 *F, u
     cudaMemsetAsync(ccnt, 0, (size_t)C * 4, st);
     kmeans_update_kernel<<<C, 128, 0, st>>>(cent, csum, ccnt, C, D, centb, cn);
     for (uint32_t it = 0; it <= iters; ++it) {
-        for (uint32_t r0 = 0; r0 < n; r0 += brows) {
-            const uint32_t rows = std::min<uint32_t>(brows, n - r0);
-            gemm(st, err, rows, C, D, F + (size_t)r0 * D, D, 0, centb, D, 1, block.as<float>(), C, nullptr, nullptr, 0);
-            argmin_kernel<<<(rows * 32 + 255) / 256, 256, 0, st>>>(block.as<float>(), cn, rows, C, lab + r0, best + r0);
+        // assignment fused into the tensor-core product (no n x C matrix), or product + argmin for D > 256
+        if (!tc_assign(st, (int)n, (int)D, F, centb, (int)C, cn, lab, best, err)) {
+            for (uint32_t r0 = 0; r0 < n; r0 += brows) {
+                const uint32_t rows = std::min<uint32_t>(brows, n - r0);
+                gemm(st, err, rows, C, D, F + (size_t)r0 * D, D, 0, centb, D, 1, block.as<float>(), C, nullptr, nullptr,
+                     0);
+                argmin_kernel<<<(rows * 32 + 255) / 256, 256, 0, st>>>(block.as<float>(), cn, rows, C, lab + r0,
+                                                                       best + r0);
+            }
         }
         if (it == iters) break;
         cudaMemsetAsync(csum, 0, (size_t)C * D * 4, st);
