@@ -223,13 +223,13 @@ WORKLOADS = {
     "c1": dict(desc="100k x 16 uniform [0,1), euclidean; 1k queries, K=10, P=100",
                n=100_000, d=16, kind="uniform", metric="euclidean", nq=1000,
                build=dict(K=25, L=50, S=10, R=100, iterations=30, reverse=-1), P_ladder=[100], join="fp32"),
-    "c3": dict(desc="1M x 96 unit-norm mixture (1000 centres, std 0.3), angular, BF16 tensor-core join; "
-                    "10k queries, K=10", n=1_000_000, d=96, kind="sphere", centres=1000, metric="angular",
-               nq=10_000, build=dict(BUILD), P_ladder=P_LADDER, join="bf16"),
+    "c3": dict(desc="1M x 96 unit-norm mixture (1000 centres, std 0.3), angular, BF16 tensor-core join and "
+                    "BF16 search filter; 10k queries, K=10", n=1_000_000, d=96, kind="sphere", centres=1000, metric="angular",
+               nq=10_000, build=dict(BUILD), P_ladder=P_LADDER, join="bf16", search_precision="bf16"),
     "c4": dict(desc="2M x 128 mixture (256 centres); 100k queries in one launch, K from {1,10,100}, "
-                    "P from {50,100,200}; per-batch latency over 1k-query batches",
+                    "P from {50,100,200}; per-batch latency over 1k-query batches; FP8 E4M3 search filter",
                n=2_000_000, d=128, kind="mixture", centres=256, metric="euclidean", nq=100_000,
-               build=dict(BUILD), join="auto", mixed=True),
+               build=dict(BUILD), join="auto", mixed=True, search_precision="fp8"),
     "c5": dict(desc="5M x 128 mixture (4096 centres), graph K=50; router (200k training pairs) vs plain "
                     "seeded walk on 50k held-out queries, K=10", n=5_000_000, d=128, kind="mixture", centres=4096,
                metric="euclidean", nq=50_000, build=dict(BUILD),
@@ -355,6 +355,8 @@ def run_workload(args, name):
                     "batch_latency_ms": {"batch": 1000, "p50": float(np.percentile(lat, 50)),
                                          "p99": float(np.percentile(lat, 99)), "batches": len(lat)}})
         P_star = 200
+        search_kw = dict(K_per_q=Kq, P_per_q=Pq, out_ld=100)
+        search_Q = Q
     else:
         sample = Q[: w.get("plain_sample", nq)]
         st = Qt[: len(sample)]
@@ -371,6 +373,21 @@ def run_workload(args, name):
         _, t, roof = timed_search(sample, 1 if slow else args.steps, warmup=0 if slow else None, K=10, P=P_star)
         out.update({"value": len(sample) / (t / 1000), "P": P_star, "recall@10": ladder[P_star],
                     "recall_ladder": ladder, "ms_per_launch": t, "queries_timed": len(sample), "roofline": roof})
+        search_kw = dict(K=10, P=P_star)
+        search_Q = sample
+    if w.get("search_precision"):
+        # the same searches with the reduced-precision distance filter: identical results, its work and speed
+        ref = ctx.search(search_Q, **search_kw)
+        ctx.set_search_precision(w["search_precision"])
+        got, tf, _ = timed_search(search_Q, 1 if "plain_sample" in w else args.steps, **search_kw)
+        fs = ctx.search_filter_stats()
+        ctx.set_search_precision("fp32")
+        same = all((np.asarray(x).view(np.uint32) == np.asarray(y).view(np.uint32)).all() for x, y in zip(ref, got))
+        out["distance_filter"] = {"precision": w["search_precision"], "identical_results": bool(same),
+                                  "value": len(search_Q) / (tf / 1000), "ms_per_launch": tf,
+                                  "filter_evaluations": fs["approx"], "fp32_evaluations_skipped": fs["skipped"],
+                                  "max_rel_row_error": fs["max_rel_row_error"],
+                                  "mean_rel_row_error": fs["mean_rel_row_error"]}
     if Qtrain is not None:
         t0 = time.perf_counter()
         rinfo = ctx.router_train(Qtrain, clusters=1024, hidden=256, label_P=min(P_star, 4000), batch=1024,
