@@ -30,6 +30,7 @@
 #include <algorithm>
 #include <cmath>
 #include <mutex>
+#include <numeric>
 #include <random>
 #include <vector>
 #include "kg_ctx.h"
@@ -476,6 +477,7 @@ cudaError_t kmeans_run(cudaStream_t st, uint32_t *err, const __nv_bfloat16 *F, u
 
 constexpr uint32_t MIN_COMPONENT = 8;
 constexpr size_t LABEL_CHUNKS = 16;   // label searches, each with its own seeds
+constexpr int REGROUP_TOP = 8;        // most likely clusters a fine cluster may move to
 
 // Component label of every node of the context's graph (host copy in comp).
 int graph_components(kg_ctx *ctx, DevBuf &buf, std::vector<uint32_t> &comp) {
@@ -674,18 +676,13 @@ extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const flo
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "router kmeans");
     if (E == 1)
         for (uint32_t f = 0; f < Cf; ++f) hlabc[f] = (int32_t)f;
-    // the cluster of every node (coarse label of its fine cluster)
-    for (uint32_t i = 0; i < N; ++i) hlab[i] = hlabc[hlab[i]];
     // Entry nodes per cluster: those of its non-empty fine clusters, plus one
     // node of every connected component of the graph (of at least
     // MIN_COMPONENT nodes) that holds no fine entry node: a walk never leaves
     // its component, so every component needs a way in.  Such a node joins the
     // cluster its own members are assigned to.
-    std::vector<std::pair<uint32_t, uint32_t>> ent;   // (cluster, node)
-    ent.reserve(Cf + 1024);
-    for (uint32_t f = 0; f < Cf; ++f)
-        if (hkey[f] != ~0ull) ent.emplace_back((uint32_t)hlabc[f], (uint32_t)(hkey[f] & 0xFFFFFFFFu));
-    uint32_t comp_entries = 0;
+    const std::vector<int32_t> hfine(hlab.begin(), hlab.end());   // fine cluster of every node
+    std::vector<uint32_t> comp_reps;
     {
         std::vector<uint32_t> comp;
         int rc = graph_components(ctx, s1, comp);
@@ -693,30 +690,46 @@ extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const flo
         std::vector<uint32_t> size(N, 0);
         std::vector<uint8_t> covered(N, 0);
         for (uint32_t i = 0; i < ctx->gn; ++i) ++size[comp[i]];
-        for (auto &pr : ent) covered[comp[pr.second]] = 1;
+        for (uint32_t f = 0; f < Cf; ++f)
+            if (hkey[f] != ~0ull) covered[comp[(uint32_t)(hkey[f] & 0xFFFFFFFFu)]] = 1;
         for (uint32_t i = 0; i < ctx->gn; ++i)
-            if (comp[i] == i && !covered[i] && size[i] >= MIN_COMPONENT) {   // i: the component's smallest id
-                ent.emplace_back((uint32_t)hlab[i], i);
-                ++comp_entries;
-            }
+            if (comp[i] == i && !covered[i] && size[i] >= MIN_COMPONENT) comp_reps.push_back(i);   // smallest id
     }
-    std::stable_sort(ent.begin(), ent.end(),
-                     [](const std::pair<uint32_t, uint32_t> &a, const std::pair<uint32_t, uint32_t> &b) {
-                         return a.first < b.first;
-                     });
-    std::vector<uint32_t> heoff(C + 1, 0), heids(ent.size());
-    for (size_t k = 0; k < ent.size(); ++k) { ++heoff[ent[k].first + 1]; heids[k] = ent[k].second; }
-    for (uint32_t c = 0; c < C; ++c) heoff[c + 1] += heoff[c];
     uint32_t empty = 0;   // clusters without an entry node
-    for (uint32_t c = 0; c < C; ++c) empty += heoff[c + 1] == heoff[c];
-    if ((e = r.eoff.reserve((size_t)(C + 1) * 4)) != cudaSuccess ||
-        (e = r.eids.reserve(std::max<size_t>(heids.size(), 1) * 4)) != cudaSuccess)
-        return cuda_fail(ctx, e, "router alloc");
-    cudaMemcpyAsync(r.eoff.p, heoff.data(), (size_t)(C + 1) * 4, cudaMemcpyHostToDevice, st);
-    if (!heids.empty()) cudaMemcpyAsync(r.eids.p, heids.data(), heids.size() * 4, cudaMemcpyHostToDevice, st);
+    // (Re)derives every node's cluster from its fine cluster and installs the
+    // clusters' entry nodes (CSR) for the seed ranking.
+    auto install_entries = [&]() -> int {
+        for (uint32_t i = 0; i < N; ++i) hlab[i] = hlabc[hfine[i]];
+        std::vector<std::pair<uint32_t, uint32_t>> ent;   // (cluster, node)
+        ent.reserve(Cf + comp_reps.size());
+        for (uint32_t f = 0; f < Cf; ++f)
+            if (hkey[f] != ~0ull) ent.emplace_back((uint32_t)hlabc[f], (uint32_t)(hkey[f] & 0xFFFFFFFFu));
+        for (uint32_t rep : comp_reps) ent.emplace_back((uint32_t)hlab[rep], rep);
+        std::stable_sort(ent.begin(), ent.end(),
+                         [](const std::pair<uint32_t, uint32_t> &a, const std::pair<uint32_t, uint32_t> &b) {
+                             return a.first < b.first;
+                         });
+        std::vector<uint32_t> heoff(C + 1, 0), heids(ent.size());
+        for (size_t k = 0; k < ent.size(); ++k) { ++heoff[ent[k].first + 1]; heids[k] = ent[k].second; }
+        for (uint32_t c = 0; c < C; ++c) heoff[c + 1] += heoff[c];
+        empty = 0;
+        for (uint32_t c = 0; c < C; ++c) empty += heoff[c + 1] == heoff[c];
+        cudaError_t e2;
+        if ((e2 = r.eoff.reserve((size_t)(C + 1) * 4)) != cudaSuccess ||
+            (e2 = r.eids.reserve(std::max<size_t>(heids.size(), 1) * 4)) != cudaSuccess)
+            return cuda_fail(ctx, e2, "router alloc");
+        cudaMemcpyAsync(r.eoff.p, heoff.data(), (size_t)(C + 1) * 4, cudaMemcpyHostToDevice, st);
+        if (!heids.empty()) cudaMemcpyAsync(r.eids.p, heids.data(), heids.size() * 4, cudaMemcpyHostToDevice, st);
+        if ((e2 = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e2, "router entries");
+        r.entries_total = (uint32_t)heids.size();
+        r.component_entries = (uint32_t)comp_reps.size();
+        return KG_OK;
+    };
+    {
+        int rc = install_entries();
+        if (rc != KG_OK) return rc;
+    }
     r.probe = std::max(1u, std::min(p->probe, C));
-    r.entries_total = (uint32_t)heids.size();
-    r.component_entries = comp_entries;
 
     // 4. training set: query features and the cluster of each query's best node
     std::vector<int32_t> ylab(ntrain);
@@ -808,6 +821,44 @@ extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const flo
             topd[i] = sd[i * ld];
             cnt[i] = 1;
             ylab[i] = hlab[node];
+        }
+        // Regrouping: every fine cluster moves to the cluster the network
+        // predicts for its centroid (the first of its REGROUP_TOP most likely
+        // that is not full), so the clusters become groups the network can tell
+        // apart; the labels follow and training continues.
+        if (E > 1) {
+            DevBuf dtop;
+            cudaError_t e2 = dtop.reserve((size_t)Cf * REGROUP_TOP * 4);
+            if (e2 != cudaSuccess) return cuda_fail(ctx, e2, "router alloc");
+            for (uint32_t c0 = 0; c0 < Cf; c0 += r.batch) {
+                const uint32_t bs = std::min<uint32_t>(r.batch, Cf - c0);
+                cudaMemcpyAsync(r.X.p, centf + (size_t)c0 * D, (size_t)bs * D * 2, cudaMemcpyDeviceToDevice, st);
+                forward(st, r, (int)bs);
+                topm_kernel<<<((int)bs * 32 + 255) / 256, 256, 0, st>>>(r.Z.as<float>(), (int)bs, (int)C, REGROUP_TOP,
+                                                                         nullptr, dtop.as<uint32_t>() + (size_t)c0 * REGROUP_TOP,
+                                                                         REGROUP_TOP);
+            }
+            std::vector<uint32_t> htop((size_t)Cf * REGROUP_TOP);
+            cudaMemcpyAsync(htop.data(), dtop.p, htop.size() * 4, cudaMemcpyDeviceToHost, st);
+            e2 = cudaStreamSynchronize(st);
+            dtop.release();
+            if (e2 != cudaSuccess) return cuda_fail(ctx, e2, "router regroup");
+            const uint32_t cap = (Cf + C - 1) / C * 3 / 2 + 1;
+            std::vector<uint32_t> load(C, 0), forder(Cf);
+            std::iota(forder.begin(), forder.end(), 0u);
+            std::shuffle(forder.begin(), forder.end(), rng);
+            std::vector<int32_t> nl(hlabc);
+            for (uint32_t f : forder) {
+                int pick = -1;
+                for (int t = 0; t < REGROUP_TOP && pick < 0; ++t)
+                    if (load[htop[(size_t)f * REGROUP_TOP + t]] < cap) pick = (int)htop[(size_t)f * REGROUP_TOP + t];
+                if (pick < 0) pick = hlabc[f];
+                nl[f] = pick;
+                ++load[pick];
+            }
+            hlabc.swap(nl);
+            if ((rc = install_entries()) != KG_OK) return rc;
+            for (size_t i = 0; i < ntrain; ++i) ylab[i] = cnt[i] ? hlab[top[i] < N ? top[i] : 0] : 0;
         }
         if ((rc = run_epochs(p->epochs)) != KG_OK) return rc;
     }
