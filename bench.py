@@ -144,6 +144,16 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def hbm_peak():
+    """HBM copy bandwidth (GB/s) the roofline divides by: the measured figure in
+    MEASURED_PEAKS.json when present, else the pool's earlier measurement."""
+    try:
+        v = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+        return v, "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback (6650 GB/s, an earlier copy-bandwidth measurement on this pool)"
+
+
 def max_over_ranks(x, dist, world, device):
     """Max of a per-rank float over all ranks (every rank takes the same collective step)."""
     import torch
@@ -308,12 +318,7 @@ def run_workload(args, name):
     Xt = torch.as_tensor(X, dtype=torch.float64, device="cuda")
     Qt = torch.as_tensor(Q, dtype=torch.float64, device="cuda")
     gt_d, _ = exact_topk_fp64_chunked(Xt, Qt, 100 if w.get("mixed") else 10, torch)
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except OSError:
-        pass
-    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    hbm, peak_source = hbm_peak()
     row_bytes = 4 * d + 4
 
     def timed_search(Qs, reps, warmup=None, **kw):
@@ -326,7 +331,7 @@ def run_workload(args, name):
         ev, adj = ctx.search_work()
         t = sum(ms) / len(ms)
         gbs = (ev * row_bytes + adj * 4) / (t / 1000) / 1e9
-        return r, t, {"achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm}
+        return r, t, {"achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm, "peak_source": peak_source}
 
     if w.get("mixed"):
         rng = np.random.default_rng(4)
@@ -662,12 +667,7 @@ def main():
     # roofline of the search kernel: algorithmic bytes per launch / launch time
     bytes_per_launch = evals * (DIM * 4 + 4) + adj * 4
     achieved = bytes_per_launch / (tot_ms / args.steps / 1000) / 1e9
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except OSError:
-        pass
-    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    hbm, peak_source = hbm_peak()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -723,9 +723,11 @@ def main():
                 "roofline": ({"bound": "hbm", "kernel": "search_kernel (router-seeded)",
                               "achieved": router["roofline"]["achieved"], "peak": hbm, "unit": "GB/s",
                               "frac": router["roofline"]["frac"], "traffic": ROUTER_SEARCH_DRAM_BYTES_PER_LAUNCH,
+                              "peak_source": peak_source,
                               "algorithmic_bytes_per_launch": router["algorithmic_bytes_per_launch"]} if best_router else
                              {"bound": "hbm", "kernel": "search_kernel", "achieved": achieved, "peak": hbm,
                               "unit": "GB/s", "frac": achieved / hbm, "traffic": SEARCH_DRAM_BYTES_PER_LAUNCH,
+                              "peak_source": peak_source,
                               "algorithmic_bytes_per_launch": int(bytes_per_launch)}),
                 "clocks": clk.summary(), "cpu_baseline": cpu}
         print(json.dumps(line))
