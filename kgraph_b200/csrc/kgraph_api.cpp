@@ -259,6 +259,14 @@ public:
         if (r != KG_OK) throw_code(r, kg_last_error(ctx));
     }
 
+    void *native_context(IndexOracle const &oracle) override {
+        std::lock_guard<std::mutex> g(mu);
+        auto const *dense = dynamic_cast<DenseIndexOracle const *>(&oracle);
+        if (!dense) throw invalid_argument("kgraph-b200 needs a dense oracle");
+        bind(ctx, binding, dense->dense(), false);
+        return ctx;
+    }
+
     void get_nn(unsigned id, unsigned *nns, float *dist, unsigned *pM, unsigned *pL) const override {
         std::lock_guard<std::mutex> g(mu);
         refresh();

@@ -50,6 +50,13 @@ def test_python_module_errors_match_reference():
     assert kgraph.arch["name"] == "sm_100a"
 
 
+def test_python_module_has_the_extensions():
+    import kgraph_b200 as kgraph
+    for name in ("train_router", "set_search_precision", "autotune", "search", "build", "load", "save"):
+        assert hasattr(kgraph.KGraph, name), name
+    assert "router" in kgraph.KGraph.search.__doc__
+
+
 def test_context_creation_fails_cleanly_without_gpu():
     import torch
     if torch.cuda.is_available():
