@@ -526,6 +526,11 @@ def main():
         if ladder[P] >= TARGET:
             P_star = P
             break
+    # every rank runs the same P (the largest any rank needs), so ranks take the same steps
+    P_star = int(max_over_ranks(P_star, dist, world, "cuda"))
+    if P_star not in ladder:
+        ids, _, _, _ = ctx.search(Q, K=10, P=P_star)
+        ladder[P_star] = recall_at(ids, Xt, Qt, gt_d, 10, torch)
     ids100, _, _, _ = ctx.search(Q, K=100, P=max(P_star, 100))
     recall100 = recall_at(ids100, Xt, Qt, gt_d, 100, torch)
     # launch shape of the search kernel picked by the library's autotuner on a sample
@@ -599,6 +604,14 @@ def main():
             if r_ladder[P] >= TARGET:
                 P_r = P
                 break
+        # all ranks agree on the router's P (or that the target was missed), so they take the same
+        # collective steps below
+        NOT_REACHED = ROUTER_P_LADDER[-1] + 1
+        agreed = int(max_over_ranks(NOT_REACHED if P_r is None else P_r, dist, world, "cuda"))
+        P_r = None if agreed == NOT_REACHED else agreed
+        if P_r is not None and P_r not in r_ladder:
+            ids, _, _, _ = ctx.search(Q, K=10, P=P_r, init=ROUTER_SEEDS, init_ids=seeds)
+            r_ladder[P_r] = recall_at(ids, Xt2, Qt, gt_d, 10, torch)
         if P_r is not None:
             rparams = capi.SearchParams(10, 0, P_r, 10, 1, 1e30, 1998, ROUTER_SEEDS)
             tune_router = ctx.search_autotune(Q, K=10, P=P_r, init=ROUTER_SEEDS, init_ids=seeds)
