@@ -497,21 +497,28 @@ def main():
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
-    X, Q, Qtrain = make_data(n=args.n, rank=rank, ntrain=args.router_train)
+    X, Q, *rest = make_data(n=args.n, rank=rank, ntrain=args.router_train)
+    Qtrain = rest[0] if rest else None
     ctx = capi.Context(local)
     capi.set_verbosity(0)
     ctx.set_data(X, "euclidean")
     # build (timed on the device by the library's own CUDA events): the first
     # build of a process also pays one-time costs (module loading, state
-    # allocation, graph capture), so the reported build is the second one
+    # allocation, graph capture), so it is reported apart from the warm ones
     t0 = time.perf_counter()
     ctx.build(**BUILD)
     cold_wall = time.perf_counter() - t0
     cold_ms, _ = ctx.timing()
-    t0 = time.perf_counter()
-    info = ctx.build(**BUILD)
-    build_wall = time.perf_counter() - t0
-    build_ms, _ = ctx.timing()
+    # the warm build, three times (the build is nondeterministic under racy inserts, like the
+    # reference's): the median is reported, all three are listed
+    builds = []
+    torch.cuda.nvtx.range_push("build_timed")   # ncu selects the build's launches by this range
+    for _ in range(3):
+        t0 = time.perf_counter()
+        info = ctx.build(**BUILD)
+        builds.append((ctx.timing()[0], time.perf_counter() - t0, info))
+    torch.cuda.nvtx.range_pop()
+    build_ms, build_wall, info = sorted(builds, key=lambda b: b[0])[1]
     build_graphs = ctx.build_graph_launches()
 
     # recall ladder on the GPU-built graph; FP64 ground truth on the GPU
@@ -725,6 +732,7 @@ def main():
                 "recall@10": ladder[P_star], "recall_ladder": ladder, "recall@100_at_P": recall100,
                 "build": {"seconds": build_ms / 1000, "wall_s": build_wall, "info": info,
                           "first_build_seconds": cold_ms / 1000, "first_build_wall_s": cold_wall,
+                          "warm_builds_seconds": [b[0] / 1000 for b in builds],
                           "graph_launches": build_graphs},
                 # per step: the queries in, and the ids buffer in (the library keeps a caller's entries
                 # beyond each query's result count, as the reference does); ids, distances, counts out

@@ -168,8 +168,47 @@ __global__ void __launch_bounds__(256) init_kernel(BuildState s) {
     }
 }
 
+// Two pair distances sharing row j (4-lane group): dist(i0, j) and dist(i1, j)
+// with the bits of pair_dist (the canonical distance is symmetric bit for bit:
+// products, squares of differences and the norm sum all commute), row j read
+// once for both.
+__device__ __forceinline__ void pair_dist_shared(const DataView &D, uint32_t j, uint32_t i0, uint32_t i1, int t,
+                                                 unsigned mask, float &d0, float &d1) {
+    const float *rj = D.X + (size_t)j * D.ld, *r0 = D.X + (size_t)i0 * D.ld, *r1 = D.X + (size_t)i1 * D.ld;
+    float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = make_float4(0.f, 0.f, 0.f, 0.f);
+    const int chunks = (int)D.d >> 4;
+    for (int c = 0; c < chunks; ++c) {
+        const float4 y = ld4(rj + 16 * c + 4 * t);
+        lane_acc(a0, ld4(r0 + 16 * c + 4 * t), y, D.metric);
+        lane_acc(a1, ld4(r1 + 16 * c + 4 * t), y, D.metric);
+    }
+    float s0 = group4_reduce(a0, mask), s1 = group4_reduce(a1, mask);
+    int i = chunks << 4;
+    const int d = (int)D.d;
+    if (d - i >= 8) {   // the tail exactly as group4_raw
+        for (int e = i + 8; i < e; ++i) {
+            float x0 = r0[i], x1 = r1[i], y0 = rj[i], y1 = rj[i];
+            if (D.metric == METRIC_L2SQR) { x0 = __fsub_rn(x0, y0); y0 = x0; x1 = __fsub_rn(x1, y1); y1 = x1; }
+            s0 = __fadd_rn(s0, __fmul_rn(x0, y0));
+            s1 = __fadd_rn(s1, __fmul_rn(x1, y1));
+        }
+    }
+    for (; i < d; ++i) {
+        float x0 = r0[i], x1 = r1[i], y0 = rj[i], y1 = rj[i];
+        if (D.metric == METRIC_L2SQR) { x0 = __fsub_rn(x0, y0); y0 = x0; x1 = __fsub_rn(x1, y1); y1 = x1; }
+        s0 = __fmaf_rn(x0, y0, s0);
+        s1 = __fmaf_rn(x1, y1, s1);
+    }
+    if (D.metric == METRIC_L2SQR) { d0 = s0; d1 = s1; return; }
+    d0 = finish_metric(s0, D.norms[i0], D.norms[j], D.metric);
+    d1 = finish_metric(s1, D.norms[i1], D.norms[j], D.metric);
+}
+
 // ------------------------------------------------------------------ join
-// KGraphConstructor::join + Nhood::join (kgraph.cpp:740-751, 797-815).
+// KGraphConstructor::join + Nhood::join (kgraph.cpp:740-751, 797-815).  The
+// node's new entries are taken two at a time: the second one's partners are
+// the first one's minus the second itself, so each partner row read serves
+// both pairs.
 __global__ void __launch_bounds__(256) join_kernel(BuildState s) {
     const int lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
@@ -184,36 +223,51 @@ __global__ void __launch_bounds__(256) join_kernel(BuildState s) {
         const uint32_t *nw = s.nn_new + (size_t)n * s.NEWCAP;
         const uint32_t *od = s.nn_old + (size_t)n * s.OLDCAP;
         bool uu = false;
-        for (uint32_t ii = 0; ii < a; ++ii) {
-            const uint32_t iid = nw[ii];
-            const uint32_t nnn = a - ii - 1, inner = nnn + b;
+        // One pair per 4-lane group: the unlocked radius pre-test for both
+        // directions, then Nhood::parallel_try_insert of the group's pairs in turn.
+        auto settle = [&](bool valid, uint32_t x, uint32_t y, float dd) {
+            const float rx = (valid && t == 0) ? *reinterpret_cast<volatile float *>(s.radius + x) : 0.f;
+            const float ry = (valid && t == 1) ? *reinterpret_cast<volatile float *>(s.radius + y) : 0.f;
+            unsigned vm = __ballot_sync(FULL, valid && t == 0);
+            const unsigned nx = __ballot_sync(FULL, valid && t == 0 && !(dd > rx));
+            const unsigned ny = __ballot_sync(FULL, valid && t == 1 && !(dd > ry));
+            comps += __popc(vm);
+            while (vm) {
+                const int src = __ffs(vm) - 1;
+                vm &= vm - 1;
+                const uint32_t xg = __shfl_sync(FULL, x, src), yg = __shfl_sync(FULL, y, src);
+                const float dg = __shfl_sync(FULL, dd, src);
+                uint32_t r = s.Lp;
+                if (nx & (1u << src)) r = locked_insert(s, xg, yg, dg, lane);
+                if (r < s.K) uu = true;
+                if (ny & (1u << (src + 1))) locked_insert(s, yg, xg, dg, lane);
+            }
+        };
+        for (uint32_t ii = 0; ii < a; ii += 2) {
+            const bool two = ii + 1 < a;
+            uint32_t i0 = nw[ii], i1 = two ? nw[ii + 1] : 0u;
+            const bool bad0 = i0 >= N, bad1 = two && i1 >= N;
+            if (bad0 || bad1) {
+                if (lane == 0) raise_error(s.err, ERR_BAD_ID);
+                if (bad0) i0 = 0;
+                if (bad1) i1 = 0;
+            }
+            const uint32_t nnn = a - ii - 1, inner = nnn + b;   // i0's partners: new[ii+1..a) then old
             for (uint32_t base = 0; base < inner; base += 8) {
                 const uint32_t k = base + g;
-                bool valid = k < inner;
+                const bool in = k < inner;
                 const bool is_nn = k < nnn;
-                uint32_t jid = valid ? (is_nn ? nw[ii + 1 + k] : od[k - nnn]) : 0u;
-                if (valid && is_nn && jid == iid) valid = false;   // i < j by id excludes equal ids
-                uint32_t x = valid ? (is_nn ? min(iid, jid) : iid) : 0u;
-                uint32_t y = valid ? (is_nn ? max(iid, jid) : jid) : 0u;
-                if (valid && (x >= N || y >= N)) { raise_error(s.err, ERR_BAD_ID); valid = false; x = y = 0; }
-                float dd = pair_dist(s.D, x, y, t, FULL);
-                // parallel unlocked radius pre-test for both directions
-                float rx = (valid && t == 0) ? *reinterpret_cast<volatile float *>(s.radius + x) : 0.f;
-                float ry = (valid && t == 1) ? *reinterpret_cast<volatile float *>(s.radius + y) : 0.f;
-                unsigned vm = __ballot_sync(FULL, valid && t == 0);
-                unsigned nx = __ballot_sync(FULL, valid && t == 0 && !(dd > rx));
-                unsigned ny = __ballot_sync(FULL, valid && t == 1 && !(dd > ry));
-                comps += __popc(vm);
-                while (vm) {
-                    const int src = __ffs(vm) - 1;
-                    vm &= vm - 1;
-                    const uint32_t xg = __shfl_sync(FULL, x, src), yg = __shfl_sync(FULL, y, src);
-                    const float dg = __shfl_sync(FULL, dd, src);
-                    uint32_t r = s.Lp;
-                    if (nx & (1u << src)) r = locked_insert(s, xg, yg, dg, lane);
-                    if (r < s.K) uu = true;
-                    if (ny & (1u << (src + 1))) locked_insert(s, yg, xg, dg, lane);
-                }
+                uint32_t jid = in ? (is_nn ? nw[ii + 1 + k] : od[k - nnn]) : 0u;
+                const bool badj = in && jid >= N;
+                if (badj) { raise_error(s.err, ERR_BAD_ID); jid = 0; }
+                // i < j by id excludes equal ids; i1's partners start after itself (k >= 1)
+                const bool v0 = in && !badj && !bad0 && !(is_nn && jid == i0);
+                const bool v1 = two && in && k >= 1 && !badj && !bad1 && !(is_nn && jid == i1);
+                float d0, d1;
+                pair_dist_shared(s.D, jid, i0, i1, t, FULL, d0, d1);
+                settle(v0, v0 ? (is_nn ? min(i0, jid) : i0) : 0u, v0 ? (is_nn ? max(i0, jid) : jid) : 0u, d0);
+                if (two)
+                    settle(v1, v1 ? (is_nn ? min(i1, jid) : i1) : 0u, v1 ? (is_nn ? max(i1, jid) : jid) : 0u, d1);
             }
         }
         if (lane == 0) s.found[n] = uu ? 1u : 0u;
