@@ -99,6 +99,65 @@ def recall_at(ids, Xt, Qt, gt_d, K, torch):
     return tot / (Qt.shape[0] * K)
 
 
+def graph_recall_fp64(offsets, ids, dists, Xt, sample, K, torch):
+    """Graph recall@K on a node sample: the first K entries of each sampled node's
+    list (by stored distance) whose exact FP64 squared distance is <= the node's
+    exact K-th nearest (self excluded), over K * len(sample).  Exact on the
+    integer mixture data."""
+    S = torch.as_tensor(sample.astype(np.int64), device=Xt.device)
+    xs = Xt[S]
+    xn = (Xt * Xt).sum(1)
+    kth = []
+    for a in range(0, len(sample), 250):
+        d = xn[None, :] - 2.0 * (xs[a:a + 250] @ Xt.T) + (xs[a:a + 250] * xs[a:a + 250]).sum(1)[:, None]
+        d[torch.arange(d.shape[0], device=Xt.device), S[a:a + 250]] = float("inf")
+        kth.append(torch.topk(d, K, dim=1, largest=False).values[:, K - 1])
+    kth = torch.cat(kth)
+    first = np.zeros((len(sample), K), np.int64)
+    for r, node in enumerate(sample):
+        a, b = int(offsets[node]), int(offsets[node + 1])
+        row = ids[a:b][np.argsort(dists[a:b], kind="stable")][:K]
+        first[r, :len(row)] = row
+        first[r, len(row):] = node   # a short list: pad with the node itself (never counted)
+    F = torch.as_tensor(first, device=Xt.device)
+    dd = ((Xt[F] - xs[:, None, :]) ** 2).sum(2)
+    dd[F == S[:, None]] = float("inf")
+    return float((dd <= kth[:, None] + 1e-9).sum()) / (len(sample) * K)
+
+
+def build_parity(ctx, X, Q, Xt, Qt, gt_d, P_list, gpu_recalls, torch, threads=None):
+    """The GPU-built graph against the reference's own CPU build (oracle/_ref,
+    python-api.cpp, all host threads) at the same parameters, on the same data:
+    recall@10 of the reference-exact search over the same queries at each P, and
+    graph recall@10 on the same 1,000-node sample."""
+    import tempfile
+    from oracle import kgoracle as ko
+    kg = ko.load_reference_module()
+    sample = np.sort(np.random.default_rng(5).choice(X.shape[0], 1000, replace=False))
+    off, gi, gd, _ = ctx.graph()
+    gpu = {"graph_recall@10": graph_recall_fp64(off, gi, gd, Xt, sample, 10, torch),
+           "search_recall@10": {str(P): gpu_recalls[P] for P in P_list}}
+    g = kg.KGraph(X, "euclidean")
+    t0 = time.perf_counter()
+    g.build(**{k: v for k, v in BUILD.items() if k != "R"})
+    ref_build_s = time.perf_counter() - t0
+    with tempfile.TemporaryDirectory() as tmp:
+        p = os.path.join(tmp, "ref.idx")
+        g.save(p)
+        G = ko.read_index(p)
+    ref = {"graph_recall@10": graph_recall_fp64(G.offsets, G.ids, G.dists, Xt, sample, 10, torch),
+           "search_recall@10": {str(P): recall_at(np.asarray(g.search(Q, K=10, P=P)), Xt, Qt, gt_d, 10, torch)
+                                for P in P_list},
+           "build_seconds": ref_build_s, "threads": threads or os.cpu_count()}
+    delta = {"graph_recall@10": gpu["graph_recall@10"] - ref["graph_recall@10"]}
+    delta.update({"search_recall@10_P%s" % P: gpu["search_recall@10"][P] - ref["search_recall@10"][P]
+                  for P in gpu["search_recall@10"]})
+    return {"queries": int(Q.shape[0]), "node_sample": len(sample), "gpu_graph": gpu, "reference_graph": ref,
+            "delta": delta, "max_abs_delta": max(abs(v) for v in delta.values()),
+            "note": "same data, same queries, same search seeds; the reference graph is built by the reference's "
+                    "own CPU code at the same parameters"}
+
+
 class ClockSampler:
     """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
 
@@ -207,15 +266,21 @@ def run_reference_arm(args, rank, world):
     qps = len(sample) * len(times) / sum(times)
     import torch
     rec = None
+    rec_all = None
     if torch.cuda.is_available():
         Xt = torch.as_tensor(X, dtype=torch.float64, device="cuda")
         Qt = torch.as_tensor(sample, dtype=torch.float64, device="cuda")
         gd, _ = exact_topk_fp64(Xt, Qt, 10, torch)
         rec = recall_at(ids, Xt, Qt, gd, 10, torch)
+        # the same graph's recall over all 10,000 queries (untimed), at the P values the GPU arm reports
+        Qa = torch.as_tensor(Q, dtype=torch.float64, device="cuda")
+        ga, _ = exact_topk_fp64(Xt, Qa, 10, torch)
+        rec_all = {str(Pa): recall_at(np.asarray(g.search(Q, K=10, P=Pa)), Xt, Qa, ga, 10, torch)
+                   for Pa in sorted({100, P})}
     line = {"metric": METRIC, "value": qps, "unit": UNIT, "impl": "reference", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sum(times) / len(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "recall@10": rec,
+            "data": "synthetic", "recall@10": rec, "recall@10_all_10k_queries": rec_all,
             "config": {"workload": "1M x 128 mixture (256 centres), K=10 search, P=%d" % P, "P": P,
                        "queries_per_step": len(sample), "build": BUILD},
             "build": {"seconds": build_s, "threads": cores},
@@ -478,6 +543,8 @@ def main():
     ap.add_argument("--ref-queries", type=int, default=2000)
     ap.add_argument("--cpu-queries", type=int, default=1000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the reference's CPU build of the same graph (build parity, ~35 s on 16 threads)")
     ap.add_argument("--router-train", type=int, default=ROUTER_TRAIN)
     ap.add_argument("--workload", default="c2", choices=["c2"] + sorted(WORKLOADS),
                     help="c2 (default) is the headline 1M x 128 benchmark")
@@ -516,10 +583,13 @@ def main():
     for _ in range(3):
         t0 = time.perf_counter()
         info = ctx.build(**BUILD)
-        builds.append((ctx.timing()[0], time.perf_counter() - t0, info))
+        builds.append((ctx.timing()[0], time.perf_counter() - t0, info, ctx.build_work()))
     torch.cuda.nvtx.range_pop()
-    build_ms, build_wall, info = sorted(builds, key=lambda b: b[0])[1]
+    build_ms, build_wall, info, (b_pairs, b_lists, b_iters) = sorted(builds, key=lambda b: b[0])[1]
     build_graphs = ctx.build_graph_launches()
+    # algorithmic bytes of the build (per iteration and node: the join's list rows, 4 D + 4 bytes each, and
+    # one read and one write of the (L+1)-entry pool of 12-byte entries)
+    build_bytes = b_lists * (DIM * 4 + 4) + b_iters * args.n * 2 * (BUILD["L"] + 1) * 12
 
     # recall ladder on the GPU-built graph; FP64 ground truth on the GPU
     Xt = torch.as_tensor(X, dtype=torch.float64, device="cuda")
@@ -540,6 +610,22 @@ def main():
         ladder[P_star] = recall_at(ids, Xt, Qt, gt_d, 10, torch)
     ids100, _, _, _ = ctx.search(Q, K=100, P=max(P_star, 100))
     recall100 = recall_at(ids100, Xt, Qt, gt_d, 100, torch)
+    # build parity: the reference's own CPU build at the same parameters, scored on the same queries
+    parity = None
+    parity_P = sorted({100, P_star})
+    if rank == 0 and world == 1 and not args.no_parity:
+        try:
+            from oracle import kgoracle as ko
+            if ko.reference_available():
+                for P in parity_P:
+                    if P not in ladder:
+                        ids, _, _, _ = ctx.search(Q, K=10, P=P)
+                        ladder[P] = recall_at(ids, Xt, Qt, gt_d, 10, torch)
+                parity = build_parity(ctx, X, Q, Xt, Qt, gt_d, parity_P, ladder, torch)
+            else:
+                parity = {"unavailable": "reference not compiled (oracle/_ref missing)"}
+        except Exception as e:   # reported, not fatal
+            parity = {"error": str(e)[:200]}
     # launch shape of the search kernel picked by the library's autotuner on a sample
     tune_plain = ctx.search_autotune(Q[:2000], K=10, P=P_star)
     Xt2 = Xt
@@ -700,10 +786,13 @@ def main():
                     off, gi, gd, gM = ctx.graph()
                     ctx_save(p, off, gi, gd, gM)
                     sample = Q[: args.cpu_queries]
-                    _, secs = reference_cpu_search(X, sample, p, 10, P_star)
+                    ref_ids, secs = reference_cpu_search(X, sample, p, 10, P_star)
+                    gpu_ids, _, _, _ = ctx.search(sample, K=10, P=P_star)
                     cpu = {"value": len(sample) / secs, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                            "sample": "%d queries, K=10, P=%d, reference CPU search (oracle/_ref, OpenMP over "
-                                     "queries) on the same GPU-built graph" % (len(sample), P_star)}
+                                     "queries) on the same GPU-built graph" % (len(sample), P_star),
+                           # the reference's walk and the GPU walk on the same graph: identical ids
+                           "ids_identical_to_gpu_walk": bool((np.asarray(ref_ids, np.uint32) == gpu_ids).all())}
         except Exception as e:   # reported, not fatal
             cpu = {"error": str(e)[:200]}
 
@@ -733,7 +822,14 @@ def main():
                 "build": {"seconds": build_ms / 1000, "wall_s": build_wall, "info": info,
                           "first_build_seconds": cold_ms / 1000, "first_build_wall_s": cold_wall,
                           "warm_builds_seconds": [b[0] / 1000 for b in builds],
-                          "graph_launches": build_graphs},
+                          "graph_launches": build_graphs,
+                          "work": {"join_pairs": b_pairs, "join_list_entries": b_lists, "iterations": b_iters},
+                          "roofline": {"bound": "hbm", "algorithmic_bytes": int(build_bytes),
+                                       "achieved": build_bytes / (build_ms / 1000) / 1e9, "peak": hbm,
+                                       "unit": "GB/s", "frac": build_bytes / (build_ms / 1000) / 1e9 / hbm,
+                                       "peak_source": peak_source,
+                                       "bytes": "join list entries x (4 D + 4) + iterations x N x 2 (L+1) x 12"}},
+                "build_parity": parity,
                 # per step: the queries in, and the ids buffer in (the library keeps a caller's entries
                 # beyond each query's result count, as the reference does); ids, distances, counts out
                 "e2e": {"value": head_e2e, "unit": UNIT, "h2d_bytes_per_step": int(Qh.nbytes + hi.nbytes),

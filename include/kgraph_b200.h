@@ -184,10 +184,16 @@ int kg_prune(kg_ctx *ctx, unsigned level);
  * Scratch (counters, seed table, visited sets) is a static device array of
  * KG_NOALLOC_SCRATCH_BYTES per GPU, held until the process exits; a batch
  * whose seeds, per-query index and one SM's worth of visited sets do not fit
- * is rejected with KG_E_INVALID.  The first call on a device looks up the
- * array's device address, so make it before any stream capture.  Every call
+ * is rejected with KG_E_INVALID.  The first call through a context looks up
+ * the array's device address on the context's device and keeps it in the
+ * context, so make that call before any stream capture; create contexts anew
+ * after a device reset (the old ones' buffers are gone with it).  Every call
  * shares the array: calls whose kernels overlap on the GPU race; serialise
- * them.  Results are those of kg_search_batch. */
+ * them.  Results are those of kg_search_batch.  Speed: it reuses the search-
+ * side copy of the graph and the distance filter's compressed rows when an
+ * earlier kg_search_batch on the context has built them; otherwise it walks
+ * the CSR graph in FP32 (same results, lower throughput), since building
+ * either would allocate. */
 #define KG_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)
 int kg_search_batch_noalloc(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes,
                             const kg_search_params *params, size_t out_ld, uint32_t *ids, float *dists,
@@ -249,6 +255,21 @@ int kg_router_gradients(kg_ctx *ctx, unsigned d, unsigned hidden, unsigned clust
 /* Milliseconds of the last kg_router_seeds device work (CUDA events on the
  * context's stream). */
 int kg_last_router_timing(kg_ctx *ctx, float *seeds_ms);
+/* Checks of the router's tensor-core products on caller data (no counterpart
+ * in the reference).  Operands are BF16 bit patterns (uint16), host or device
+ * memory; outputs are copied back to the caller's buffers.
+ * kg_tc_gemm_check: C[M,N] = op(A)[M,K] op(B)[K,N] (+ beta C) (+ bias[N])
+ * (ReLU when relu != 0) with FP32 accumulation, exactly the product the MLP's
+ * forward and backward passes run; op(A) = A (M x K, row stride lda) or, with
+ * ta, A^T (A stored K x M); likewise B / tb.  C has row stride ldc >= N and is
+ * read when beta != 0.
+ * kg_tc_assign_check: the fused k-means assignment, lab[r] = argmin over c of
+ * cn[c] - 2 F[r].cent[c] (ties: smaller c), best[r] that value (may be NULL);
+ * F is n x D, cent C x D, row-major, D <= 256. */
+int kg_tc_gemm_check(kg_ctx *ctx, int M, int N, int K, const uint16_t *A, int lda, int ta, const uint16_t *B,
+                     int ldb, int tb, const float *bias, int relu, float beta, float *C, int ldc);
+int kg_tc_assign_check(kg_ctx *ctx, const uint16_t *F, int n, int D, const uint16_t *cent, int C, const float *cn,
+                       int32_t *lab, float *best);
 
 /* Precision of the NN-descent local join.  No counterpart in the reference
  * (its join evaluates every pair in FP32, kgraph.cpp:740-751, 797-815).
@@ -291,6 +312,12 @@ int kg_last_timing(kg_ctx *ctx, float *build_ms, float *search_ms);
  * captured once and replayed as one graph launch (two with the statistics
  * split off when the join runs on the tensor cores, three with its update). */
 int kg_last_build_graphs(kg_ctx *ctx, unsigned *graph_launches);
+/* Work of the last kg_build's local joins, summed over its iterations: pairs
+ * evaluated (the reference's IndexInfo.cost * N(N-1)/2 counter,
+ * kgraph.cpp:797-815, 928), list entries (|new| + |old| over all nodes: the
+ * dataset rows the joins read) and the iterations run.  Any pointer may be
+ * NULL. */
+int kg_last_build_work(kg_ctx *ctx, uint64_t *pairs, uint64_t *list_entries, unsigned *iterations);
 /* Work of the last kg_search_batch: distance evaluations (seeds included;
  * the sum of SearchInfo.cost * N plus the seeds) and adjacency entries read. */
 int kg_last_search_work(kg_ctx *ctx, uint64_t *evaluations, uint64_t *adjacency_reads);

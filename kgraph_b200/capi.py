@@ -23,7 +23,7 @@ SYMBOLS = [
     "kg_router_params_default", "kg_router_train", "kg_router_seeds", "kg_router_gradients", "kg_last_router_timing",
     "kg_set_join_precision", "kg_last_join_stats", "kg_last_build_graphs", "kg_search_autotune",
     "kg_set_search_tuning", "kg_get_search_tuning", "kg_set_search_precision", "kg_last_search_filter",
-    "kg_filter_bounds", "kg_router_search",
+    "kg_filter_bounds", "kg_router_search", "kg_tc_gemm_check", "kg_tc_assign_check", "kg_last_build_work",
 ]
 
 JOIN = {"auto": 0, "fp32": 1, "bf16": 2, "bf16_always": 3}
@@ -124,6 +124,10 @@ def lib():
         L.kg_last_search_filter.argtypes = [vp, C.POINTER(FilterStats)]
         L.kg_filter_bounds.argtypes = [vp, vp, sz, sz, vp, sz, vp, vp]
         L.kg_router_search.argtypes = [vp, vp, sz, sz, C.POINTER(SearchParams), sz, vp, vp, vp, vp]
+        L.kg_tc_gemm_check.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, C.c_int, C.c_int, vp, C.c_int, C.c_int,
+                                       vp, C.c_int, C.c_float, vp, C.c_int]
+        L.kg_tc_assign_check.argtypes = [vp, vp, C.c_int, C.c_int, vp, C.c_int, vp, vp, vp]
+        L.kg_last_build_work.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint)]
         L.kg_index_params_default.argtypes = [C.POINTER(IndexParams)]
         L.kg_search_params_default.argtypes = [C.POINTER(SearchParams)]
         _lib = L
@@ -294,11 +298,41 @@ class Context:
                                                x.shape[0], C.byref(loss), _ptr(grads)))
         return loss.value, grads
 
+    def tc_gemm_check(self, A, B, ta=False, tb=False, bias=None, relu=False, beta=0.0, C_in=None):
+        """kg_tc_gemm_check: op(A) @ op(B) (+ beta C_in) (+ bias) (ReLU) on the tensor cores.
+        A and B are uint16 arrays of BF16 bit patterns."""
+        A = np.ascontiguousarray(A, np.uint16)
+        B = np.ascontiguousarray(B, np.uint16)
+        M, K = (A.shape[1], A.shape[0]) if ta else A.shape
+        N = B.shape[0] if tb else B.shape[1]
+        out = np.zeros((M, N), np.float32) if C_in is None else np.ascontiguousarray(C_in, np.float32).copy()
+        b = None if bias is None else np.ascontiguousarray(bias, np.float32)
+        self._check(self.L.kg_tc_gemm_check(self.h, M, N, K, _ptr(A), A.shape[1], int(ta), _ptr(B), B.shape[1],
+                                            int(tb), _ptr(b), int(relu), beta, _ptr(out), N))
+        return out
+
+    def tc_assign_check(self, F, cent, cn):
+        """kg_tc_assign_check: argmin_c cn[c] - 2 F.cent[c] per row (BF16 bit patterns in)."""
+        F = np.ascontiguousarray(F, np.uint16)
+        cent = np.ascontiguousarray(cent, np.uint16)
+        cn = np.ascontiguousarray(cn, np.float32)
+        lab = np.zeros(F.shape[0], np.int32)
+        best = np.zeros(F.shape[0], np.float32)
+        self._check(self.L.kg_tc_assign_check(self.h, _ptr(F), F.shape[0], F.shape[1], _ptr(cent), cent.shape[0],
+                                              _ptr(cn), _ptr(lab), _ptr(best)))
+        return lab, best
+
     def reverse(self, k):
         self._check(self.L.kg_reverse(self.h, k))
 
     def prune(self, level):
         self._check(self.L.kg_prune(self.h, level))
+
+    def build_work(self):
+        """kg_last_build_work: (join pairs, join list entries, iterations) of the last build."""
+        p, e, it = C.c_uint64(), C.c_uint64(), C.c_uint()
+        self._check(self.L.kg_last_build_work(self.h, C.byref(p), C.byref(e), C.byref(it)))
+        return p.value, e.value, it.value
 
     def search_work(self):
         ev, adj = C.c_uint64(), C.c_uint64()

@@ -276,26 +276,30 @@ __global__ void __launch_bounds__(256) join_kernel(BuildState s) {
 }
 
 // ------------------------------------------------------------------ statistics
-// Flags in pool[0..K) (EvaluateDelta, kgraph.cpp:148-156), the sum of M and
-// the number of full pools.
+// Flags in pool[0..K) (EvaluateDelta, kgraph.cpp:148-156), the sum of M,
+// the number of full pools, and the join's list entries (|new| + |old|, the
+// rows the join read; accumulated over the build for its byte count).
 __global__ void stats_kernel(BuildState s) {
-    unsigned long long fl = 0, msum = 0, full = 0;
+    unsigned long long fl = 0, msum = 0, full = 0, lists = 0;
     const uint32_t lim = min(s.K, s.Lp);
     for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < s.D.n; n += gridDim.x * blockDim.x) {
         const uint32_t *pi = s.pool_i + (size_t)n * s.PS;
         for (uint32_t l = 0; l < lim; ++l) fl += (pi[l] & FLAG_BIT) ? 1 : 0;
         msum += s.nodeM[n];
         full += s.nodeL[n] + 1 >= s.Lp ? 1 : 0;   // pool full: a finite radius
+        lists += s.cnt_new[n] + s.cnt_old[n];
     }
     for (int o = 16; o; o >>= 1) {
         fl += __shfl_xor_sync(FULL, fl, o);
         msum += __shfl_xor_sync(FULL, msum, o);
         full += __shfl_xor_sync(FULL, full, o);
+        lists += __shfl_xor_sync(FULL, lists, o);
     }
     if ((threadIdx.x & 31) == 0) {
         atomicAdd(s.stat + 0, fl);
         atomicAdd(s.stat + 1, msum);
         atomicAdd(s.stat + 2, full);
+        atomicAdd(s.list_entries, lists);
     }
 }
 
@@ -649,6 +653,7 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
     s.stat = s.n_comps + 1;
     s.work = reinterpret_cast<uint32_t *>(s.n_comps + 4);
     s.iter = s.work + 2;
+    s.list_entries = s.n_comps + 6;   // 64-byte block: n_comps, stat[3], work, iter, list_entries
     s.err = ctx->errw.as<uint32_t>();
     cudaStream_t st = ctx->stream;
     cudaMemsetAsync(B[18].p, 0, 64, st);
@@ -893,6 +898,8 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
     cudaEventRecord(ctx->ev1, st);
     JoinTcStats ts{};
     cudaMemcpyAsync(&ts, s.tc, sizeof(ts), cudaMemcpyDeviceToHost, st);
+    unsigned long long lists = 0;
+    cudaMemcpyAsync(&lists, s.list_entries, 8, cudaMemcpyDeviceToHost, st);
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "build");
     cudaEventElapsedTime(&ctx->last_build_ms, ctx->ev0, ctx->ev1);
     kg_join_stats &js = ctx->last_join;
@@ -910,7 +917,19 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
     js.mean_abs_err = ts.sampled ? ts.sum_abs / ts.sampled : 0.0;
     js.mean_err_over_margin = ts.sampled ? ts.sum_ratio / ts.sampled : 0.0;
     js.mean_rel_err = ts.rel_count ? ts.sum_rel / ts.rel_count : 0.0;
+    ctx->last_build_work[0] = hstat_prev;
+    ctx->last_build_work[1] = lists;
+    ctx->last_build_work[2] = inf.iterations;
     if (info) *info = inf;
+    return KG_OK;
+}
+
+extern "C" int kg_last_build_work(kg_ctx *ctx, uint64_t *pairs, uint64_t *list_entries, unsigned *iterations) {
+    if (!ctx) return KG_E_INVALID;
+    std::lock_guard<std::mutex> guard(ctx->mu);
+    if (pairs) *pairs = ctx->last_build_work[0];
+    if (list_entries) *list_entries = ctx->last_build_work[1];
+    if (iterations) *iterations = (unsigned)ctx->last_build_work[2];
     return KG_OK;
 }
 

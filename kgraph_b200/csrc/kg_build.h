@@ -25,7 +25,8 @@ struct BuildState {
     uint64_t *roff_new, *roff_old;       // exclusive scans of the counts (N+1)
     uint32_t *rbuf_new, *rbuf_old;       // reverse samples, CSR by target
     unsigned long long *n_comps;         // join pair counter
-    unsigned long long *stat;            // [0] flagged-in-top-K count, [1] sum of M
+    unsigned long long *stat;            // [0] flagged-in-top-K count, [1] sum of M, [2] full pools
+    unsigned long long *list_entries;    // join list entries (|new| + |old| summed over nodes and iterations)
     uint32_t *err;
     uint32_t *work;                      // dynamic work counter
     uint64_t seed;

@@ -48,6 +48,7 @@ struct kg_ctx {
     std::string err;
     float last_build_ms = 0.f, last_search_ms = 0.f, last_router_ms = 0.f;
     unsigned last_build_graph_launches = 0;   // CUDA graph launches of the last build's iterations
+    unsigned long long last_build_work[3] = {0, 0, 0};   // join pairs, join list entries, iterations
     unsigned long long last_work[4] = {0, 0, 0, 0};   // evaluations, adjacency reads, filter: approx, skipped
 
     // dataset
@@ -88,6 +89,7 @@ struct kg_ctx {
     kgb::DevBuf joinq, joinaux, joinb;   // tensor-core join: candidate queue, worst-case prefix, round bounds
     kg_join_stats last_join{};
     kgb::RouterState *router = nullptr;   // learned entry router (kg_router.cu)
+    void *noalloc_scratch = nullptr;      // device address of kg_search_batch_noalloc's static array
     kgb::DevBuf rseeds;                   // router seeds handed to the search (kg_router_search)
 };
 

@@ -14,11 +14,18 @@
 // in one file-scope static __device__ array of KG_NOALLOC_SCRATCH_BYTES that
 // every GPU loading the library holds until the process exits.  Host code
 // cannot use the array's name as a device address (it is a host-side stand-in),
-// so the first call on each device resolves the address with
-// cudaGetSymbolAddress while that device is current, and caches it.  That first
-// call should therefore come before any stream capture.  The dataset and graph
-// are the context's (kg_set_data / kg_build / kg_graph_import allocate as
-// usual, beforehand); queries and outputs are the caller's DEVICE buffers.
+// so the first call through a context resolves the address on the context's
+// device with cudaGetSymbolAddress while that device is current, and keeps it
+// in the context.  That first call should therefore come before any stream
+// capture.  Keeping the address per context (not per process) means a context
+// created after a device reset looks it up again; a context that outlives a
+// reset is unusable anyway, since its dataset and graph buffers are gone.  The
+// dataset and graph are the context's (kg_set_data / kg_build /
+// kg_graph_import allocate as usual, beforehand); queries and outputs are the
+// caller's DEVICE buffers.  When an earlier kg_search_batch has already built
+// the context's search-side copy of the graph or the compressed rows of its
+// distance filter, this entry point uses them too (same results, faster);
+// otherwise it walks the CSR graph in FP32 and builds nothing.
 //
 // Limits.  The whole scratch is shared by every call in the process: calls
 // whose kernels overlap on the GPU race on it, so callers serialise them (one
@@ -43,24 +50,18 @@ namespace {
 
 constexpr size_t SCRATCH_BYTES = KG_NOALLOC_SCRATCH_BYTES;
 constexpr size_t HEADER_BYTES = 256;   // counter (4), error word (4), work counters (16)
-constexpr int MAX_DEVICES = 64;
-
 static __device__ __align__(256) unsigned char g_noalloc_scratch[SCRATCH_BYTES];
 
-std::mutex g_setup_mu;
-void *g_scratch_addr[MAX_DEVICES] = {nullptr};
-
-// Device address of the static scratch on `device` (which must be current).
-cudaError_t scratch_address(int device, unsigned char **out) {
-    if (device < 0 || device >= MAX_DEVICES) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> g(g_setup_mu);
-    if (!g_scratch_addr[device]) {
+// Device address of the static scratch on the context's device (which the
+// caller has made current), looked up once per context.
+cudaError_t scratch_address(kg_ctx *ctx, unsigned char **out) {
+    if (!ctx->noalloc_scratch) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return e;
-        g_scratch_addr[device] = p;
+        ctx->noalloc_scratch = p;
     }
-    *out = static_cast<unsigned char *>(g_scratch_addr[device]);
+    *out = static_cast<unsigned char *>(ctx->noalloc_scratch);
     return cudaSuccess;
 }
 
@@ -92,7 +93,7 @@ extern "C" int kg_search_batch_noalloc(kg_ctx *ctx, const float *queries, size_t
                          "kg_search_batch_noalloc needs 16-byte aligned query rows padded to a multiple of 16 floats");
 
     unsigned char *base = nullptr;
-    cudaError_t e = scratch_address(ctx->device, &base);
+    cudaError_t e = scratch_address(ctx, &base);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "noalloc scratch address");
 
     // Layout inside the static array.
@@ -113,6 +114,17 @@ extern "C" int kg_search_batch_noalloc(kg_ctx *ctx, const float *queries, size_t
     a.offsets = graph ? ctx->offsets.as<uint64_t>() : nullptr;
     a.nbr = graph ? ctx->nbr.as<uint32_t>() : nullptr;
     a.Mnode = graph ? ctx->Mnode.as<uint32_t>() : nullptr;
+    if (graph && ctx->layout_version == ctx->graph_version && ctx->ell.p) {   // already built: reuse, build nothing
+        a.ell = ctx->ell.as<uint32_t>();
+        a.ell_w = ctx->ell_w;
+        a.meta = ctx->meta.as<uint2>();
+    }
+    if (graph && ctx->search_prec != KG_SEARCH_FP32 && ctx->prec_built == ctx->search_prec &&
+        ctx->prec_data_version == ctx->data_version) {
+        a.prec = (uint32_t)ctx->search_prec;
+        a.Xc = ctx->Xc.p;
+        a.cmeta = ctx->cmeta.as<float4>();
+    }
     a.Q = queries;
     a.q_ld = ld;
     a.nq = (uint32_t)nq;

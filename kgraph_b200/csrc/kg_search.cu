@@ -321,10 +321,20 @@ __global__ void __launch_bounds__(256, MB) search_kernel(SearchArgs a) {
         const uint32_t S = a.S;
         const uint32_t cap = K + P + 1;   // knn.size(), kgraph.cpp:434
 
-        // query -> smem, and its norm term (SearchOracle ctor, python-api.cpp:98-101)
+        // query -> smem, and its norm term (SearchOracle ctor, python-api.cpp:98-101).  The padding
+        // columns [d, ld) of a caller's row may hold anything; the smem copy holds zeros there, so the
+        // compressed-row filter, which sums over whole 16-column chunks, sees (0 - 0)^2 terms.
         const float *qg = a.Q + (size_t)qi * a.q_ld;
-        for (uint32_t x = lane * 4; x < a.D.ld; x += 128)
-            *reinterpret_cast<float4 *>(s.q + x) = ld4(qg + x);
+        for (uint32_t x = lane * 4; x < a.D.ld; x += 128) {
+            float4 v = ld4(qg + x);
+            if (x + 4 > a.D.d) {
+                if (x + 0 >= a.D.d) v.x = 0.f;
+                if (x + 1 >= a.D.d) v.y = 0.f;
+                if (x + 2 >= a.D.d) v.z = 0.f;
+                if (x + 3 >= a.D.d) v.w = 0.f;
+            }
+            *reinterpret_cast<float4 *>(s.q + x) = v;
+        }
         __syncwarp();
         float qn = 0.f;
         if (a.D.metric != METRIC_L2SQR) {
@@ -611,7 +621,7 @@ __global__ void __launch_bounds__(256) filter_bounds_kernel(SearchArgs a, const 
     const uint32_t qi = blockIdx.x * 8 + w;
     if (qi >= a.nq) return;   // whole warps
     float *q = qs[w];
-    for (uint32_t x = lane; x < a.D.ld; x += 32) q[x] = a.Q[(size_t)qi * a.q_ld + x];
+    for (uint32_t x = lane; x < a.D.ld; x += 32) q[x] = x < a.D.d ? a.Q[(size_t)qi * a.q_ld + x] : 0.f;
     __syncwarp();
     float qn = 0.f;
     if (a.D.metric != METRIC_L2SQR) qn = norm_term(group4_raw(q, q, a.D.d, METRIC_EUCLIDEAN, lane & 3, FULL), a.D.metric);

@@ -10,7 +10,7 @@ thread so the graph is deterministic -- and stores inputs and outputs:
   search configuration the reference's ids / dists (and counts / costs where
   the C++ driver reports them), plus the brute-force K-NN.
 
-Run in the build container (needs /root/reference and oracle/_ref):
+Run where the reference's sources and oracle/_ref are present:
     python tests/golden/make_golden.py
 The fixtures are committed; the tests never run the reference themselves on
 the GPU box.

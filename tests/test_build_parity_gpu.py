@@ -1,0 +1,57 @@
+"""Build parity at the benchmark's graph parameters on a mid-size mixture.
+
+100,000 x 128 integer mixture (64 centres), euclidean, K=50, L=100, S=12,
+R=100, reverse=-1, 30 iterations: the graph the GPU builds must be as good as
+the reference's own multithreaded build (kgraph.cpp:886-999 through
+python-api.cpp:378-388) on the same data, within 0.005:
+
+* graph recall@10 on a fixed 2,000-node sample (first 10 entries by stored
+  distance against the exact 10-NN, self excluded, ties counted);
+* search recall@10 of the reference-exact walk (K=10, P = 50/100/300, the
+  reference's fixed seeds) over 1,000 queries from the same mixture.
+
+The reference's figures (three builds; its build is nondeterministic under
+OpenMP) are committed in tests/golden/build_parity_mix128.json by
+tests/golden/make_build_parity.py, with the judge's exact FP64 distances.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+
+def _golden():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_build_parity", os.path.join(GOLDEN, "make_build_parity.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod, json.load(open(os.path.join(GOLDEN, "build_parity_mix128.json")))
+
+
+def test_build_parity_mid_size_mixture():
+    from kgraph_b200 import capi
+    mb, gold = _golden()
+    X, Q, sample = mb.make_data()
+    node_kth = np.asarray(gold["node_kth"], np.float64)
+    query_kth = np.asarray(gold["query_kth"], np.float64)
+    ctx = capi.Context(0)
+    try:
+        capi.set_verbosity(0)
+        ctx.set_data(X, "euclidean")
+        info = ctx.build(R=100, **gold["build"])
+        off, ids, dists, M = ctx.graph()
+        g_gpu = mb.graph_recall(X, off, ids, dists, sample, node_kth)
+        refs = [b["graph_recall10"] for b in gold["reference_builds"]]
+        assert abs(g_gpu - float(np.mean(refs))) <= 0.005, (g_gpu, refs, info)
+        for P in gold["P"]:
+            r_ids, _, _, _ = ctx.search(Q, K=10, P=P)
+            s_gpu = mb.search_recall(X, Q, r_ids, query_kth)
+            s_ref = [b["search_recall10"][str(P)] for b in gold["reference_builds"]]
+            assert abs(s_gpu - float(np.mean(s_ref))) <= 0.005, (P, s_gpu, s_ref)
+    finally:
+        ctx.close()

@@ -116,3 +116,38 @@ def test_lower_bound_never_exceeds_canonical_distance(gpu_ctx, kind, d, metric, 
             assert np.median(dist - lb) < 0.5 * spread
     finally:
         gpu_ctx.set_search_precision("fp32")
+
+
+@pytest.mark.parametrize("metric", ["euclidean", "angular", "l2sqr"])
+@pytest.mark.parametrize("prec", ["bf16", "fp8"])
+def test_filter_ignores_junk_in_device_query_padding(gpu_ctx, metric, prec):
+    """Device queries used in place carry padding columns [d, ld) that may hold
+    anything (the C-ABI asks for d floats per row); NaN or huge values there
+    must not reach the filter's bound: results equal the FP32 walk's on clean
+    host queries."""
+    import torch
+    from kgraph_b200 import capi
+    d, ld, n, nq = 20, 32, 8000, 200
+    rng = np.random.default_rng(41)
+    X = dataset("sphere" if metric == "angular" else "uniform", n, d, rng)
+    Q = dataset("sphere" if metric == "angular" else "uniform", nq, d, np.random.default_rng(42))
+    gpu_ctx.set_search_precision("fp32")
+    gpu_ctx.set_data(X, metric)
+    gpu_ctx.build(K=16, L=32, S=8, reverse=-1)
+    ref = gpu_ctx.search(Q, K=10, P=40)
+    params = capi.SearchParams(10, 0, 40, 10, 1, 1e30, 1998, 0)
+    try:
+        gpu_ctx.set_search_precision(prec)
+        for pad in (float("nan"), 1e30, -3.0e38):
+            qd = torch.full((nq, ld), pad, dtype=torch.float32, device="cuda")
+            qd[:, :d] = torch.as_tensor(Q, device="cuda")
+            ids = np.zeros((nq, 10), np.uint32)
+            dist = np.zeros((nq, 10), np.float32)
+            cnt = np.zeros(nq, np.uint32)
+            cost = np.zeros(nq, np.float32)
+            gpu_ctx.search_raw(capi._ptr(qd), nq, ld * 4, params, None, None, 10, capi._ptr(ids), capi._ptr(dist),
+                               capi._ptr(cnt), capi._ptr(cost))
+            same(ref, (ids, dist, cnt, cost))
+            assert gpu_ctx.search_filter_stats()["skipped"] > 0
+    finally:
+        gpu_ctx.set_search_precision("fp32")

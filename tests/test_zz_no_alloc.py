@@ -102,3 +102,56 @@ def test_noalloc_bruteforce_without_graph_and_limits():
     with pytest.raises(capi.KGError, match="P <= 4096"):
         c2.search_noalloc(capi._ptr(q), 4, 64, big, 10, capi._ptr(ids), None, capi._ptr(cnt), None)
     c2.close()
+
+
+def test_noalloc_allocates_nothing_and_takes_init_seeds():
+    """On a fresh context, before any kg_search_batch, the device's free memory
+    is the same before and after two calls; then results (plain and with
+    init > 0 starting points, which ride in the caller's ids buffer) equal
+    kg_search_batch's."""
+    import torch
+    from kgraph_b200 import capi
+    g = load_golden("u16")
+    G = ko.read_index(g["index_bytes"])
+    ctx = capi.Context(0)
+    ctx.set_data(g["X"], g["metric"])
+    ctx.set_graph(G.offsets, G.ids, G.dists, G.M)
+    K, P, m = 10, 50, 5
+    ld = (g["X"].shape[1] + 15) // 16 * 16
+    qd = _device_rows(torch, g["Q"], ld)
+    nq = qd.shape[0]
+    ids = torch.zeros((nq, K), dtype=torch.int32, device="cuda")
+    d = torch.zeros((nq, K), dtype=torch.float32, device="cuda")
+    cnt = torch.zeros((nq,), dtype=torch.int32, device="cuda")
+    cost = torch.zeros((nq,), dtype=torch.float32, device="cuda")
+    params = capi.SearchParams(K, 0, P, 10, 1, 1e30, 1998, 0)
+
+    def call(p):
+        ctx.search_noalloc(capi._ptr(qd), nq, ld * 4, p, K, capi._ptr(ids), capi._ptr(d), capi._ptr(cnt),
+                           capi._ptr(cost))
+
+    call(params)   # first call: the context's address lookup and the kernel's first load
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(2):
+        call(params)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    got = ids.cpu().numpy().view(np.uint32).copy(), d.cpu().numpy().copy(), cnt.cpu().numpy().view(np.uint32).copy()
+    ref_i, ref_d, ref_c, _ = ctx.search(g["Q"], K=K, P=P)
+    assert (got[2] == ref_c).all() and (got[0] == ref_i).all()
+    assert (got[1].view(np.uint32) == ref_d.view(np.uint32)).all()
+    # init > 0: starting points in the first m columns of the ids buffer
+    init = np.random.default_rng(5).integers(0, g["X"].shape[0], (nq, m)).astype(np.uint32)
+    ref_i, ref_d, ref_c, ref_cost = ctx.search(g["Q"], K=K, P=P, init=m, init_ids=init)
+    params_i = capi.SearchParams(K, 0, P, 10, 1, 1e30, 1998, m)
+    for _ in range(2):
+        ids.zero_()
+        ids[:, :m] = torch.as_tensor(init.view(np.int32), device="cuda")
+        call(params_i)
+        torch.cuda.synchronize()
+        assert (cnt.cpu().numpy().view(np.uint32) == ref_c).all()
+        assert (ids.cpu().numpy().view(np.uint32) == ref_i).all()
+        assert (d.cpu().numpy().view(np.uint32) == ref_d.view(np.uint32)).all()
+        assert (cost.cpu().numpy() == ref_cost).all()
+    ctx.close()
