@@ -2,6 +2,7 @@
 
     libkgraph_b200.so   CUDA kernels + C-ABI (include/kgraph_b200.h) + C++ API (include/kgraph.h)
     _kgraph*.so         Python module (pybind11) over the C++ API
+    bin/index, bin/search   the command-line tools (the reference's index / search), over the C++ API
 
 Run as ``python -m kgraph_b200.build`` or through ``__graft_entry__.build()``.
 nvcc cross-compiles without a GPU.
@@ -73,8 +74,17 @@ def build(verbose=False):
               "-I" + pybind11.get_include(), "-I" + sysconfig.get_paths()["include"],
               "-I" + os.path.join(ROOT, "include"), src, "-o", mod,
               "-L" + PKG, "-lkgraph_b200", "-Wl,-rpath,$ORIGIN"])
+    bindir = os.path.join(PKG, "bin")
+    os.makedirs(bindir, exist_ok=True)
+    cli = os.path.join(PKG, "cli")
+    for tool in ("index", "search"):
+        src = os.path.join(cli, tool + ".cpp")
+        exe = os.path.join(bindir, tool)
+        if _stale(exe, [src, LIB, os.path.join(cli, "cli_args.h")] + HEADERS):
+            _run(["g++", "-std=c++17", "-O2", "-Wall", "-I" + os.path.join(ROOT, "include"), src, "-o", exe,
+                  "-L" + PKG, "-lkgraph_b200", "-Wl,-rpath,$ORIGIN/.."])
     if verbose:
-        print("built", LIB, mod)
+        print("built", LIB, mod, bindir)
     return LIB, mod
 
 

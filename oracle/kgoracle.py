@@ -225,12 +225,39 @@ class RefLib:
         self.lib.kgref_last_error.restype = C.c_char_p
         self.lib.kgref_set_verbosity.argtypes = [u]
         self.lib.kgref_set_threads.argtypes = [i]
+        self.lib.kgref_resave.restype = i
+        self.lib.kgref_save_lshkit.restype = i
+        self.lib.kgref_save_lshkit.argtypes = [_f32p, u, u, C.c_char_p]
+        self.lib.kgref_load_lshkit.restype = i
+        self.lib.kgref_load_lshkit.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(u), C.POINTER(u)]
+        self.lib.kgref_resave.argtypes = [C.c_char_p, C.c_char_p, i]
 
     def set_verbosity(self, v):
         self.lib.kgref_set_verbosity(v)
 
     def set_threads(self, t):
         self.lib.kgref_set_threads(t)
+
+    def save_lshkit(self, X, path):
+        """The reference's Matrix<float>::save_lshkit of X."""
+        X = np.ascontiguousarray(X, np.float32)
+        if self.lib.kgref_save_lshkit(X, X.shape[0], X.shape[1], path.encode()):
+            raise RuntimeError(self.lib.kgref_last_error().decode())
+
+    def load_lshkit(self, path):
+        """The reference's Matrix<float>::load_lshkit; returns an n x d float32 array."""
+        n, d = C.c_uint(), C.c_uint()
+        if self.lib.kgref_load_lshkit(path.encode(), None, C.byref(n), C.byref(d)):
+            raise RuntimeError(self.lib.kgref_last_error().decode())
+        out = np.zeros((n.value, d.value), np.float32)
+        if self.lib.kgref_load_lshkit(path.encode(), out.ctypes.data_as(C.c_void_p), C.byref(n), C.byref(d)):
+            raise RuntimeError(self.lib.kgref_last_error().decode())
+        return out
+
+    def resave(self, in_path, out_path, fmt):
+        """The reference loads in_path and saves it to out_path in format fmt (0, 1 no-dist, 128 text)."""
+        if self.lib.kgref_resave(in_path.encode(), out_path.encode(), fmt):
+            raise RuntimeError(self.lib.kgref_last_error().decode())
 
     def build_l2sqr(self, X, path, iterations=30, L=100, K=25, S=10, R=100, controls=100,
                     seed=1998, delta=0.002, recall=0.99, prune=0, reverse=0):

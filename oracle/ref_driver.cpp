@@ -98,6 +98,41 @@ int kgref_search_l2sqr(const float *data, unsigned n, unsigned d, const char *in
     } catch (std::exception const &e) { g_err = e.what(); return 1; }
 }
 
+// LSHKIT matrix I/O through the reference's own Matrix<float>
+// (kgraph-data.h:193-218): write n x d rows, or read a file's shape (data ==
+// NULL) and then its rows.
+int kgref_save_lshkit(const float *data, unsigned n, unsigned d, const char *path) {
+    try {
+        kgraph::Matrix<float> m;
+        fill_matrix(m, data, n, d);
+        m.save_lshkit(path);
+        return 0;
+    } catch (std::exception const &e) { g_err = e.what(); return 1; }
+}
+int kgref_load_lshkit(const char *path, float *data, unsigned *n, unsigned *d) {
+    try {
+        kgraph::Matrix<float> m;
+        m.load_lshkit(path);
+        *n = m.size();
+        *d = m.dim();
+        if (data)
+            for (unsigned i = 0; i < m.size(); ++i) std::memcpy(data + (size_t)i * m.dim(), m[i], sizeof(float) * m.dim());
+        return 0;
+    } catch (std::exception const &e) { g_err = e.what(); return 1; }
+}
+
+// Loads an index file with the reference's loader and saves it again with its
+// saver in `format` (KGraph::FORMAT_DEFAULT / FORMAT_NO_DIST / FORMAT_TEXT,
+// kgraph.cpp:291-373): the reference's own files in every format it writes.
+int kgref_resave(const char *in_path, const char *out_path, int format) {
+    try {
+        std::unique_ptr<KGraph> index(KGraph::create());
+        index->load(in_path);
+        index->save(out_path, format);
+        return 0;
+    } catch (std::exception const &e) { g_err = e.what(); return 1; }
+}
+
 // Reads an index file through the reference's loader and returns its CSR
 // form: offsets[n+1], ids/dists[E], M[n].  Call once with ids == NULL to get
 // n and E.
