@@ -583,9 +583,9 @@ def main():
     for _ in range(3):
         t0 = time.perf_counter()
         info = ctx.build(**BUILD)
-        builds.append((ctx.timing()[0], time.perf_counter() - t0, info, ctx.build_work()))
+        builds.append((ctx.timing()[0], time.perf_counter() - t0, info, ctx.build_work(), ctx.build_iterations()))
     torch.cuda.nvtx.range_pop()
-    build_ms, build_wall, info, (b_pairs, b_lists, b_iters) = sorted(builds, key=lambda b: b[0])[1]
+    build_ms, build_wall, info, (b_pairs, b_lists, b_iters), b_periter = sorted(builds, key=lambda b: b[0])[1]
     build_graphs = ctx.build_graph_launches()
     # algorithmic bytes of the build (per iteration and node: the join's list rows, 4 D + 4 bytes each, and
     # one read and one write of the (L+1)-entry pool of 12-byte entries)
@@ -824,6 +824,12 @@ def main():
                           "warm_builds_seconds": [b[0] / 1000 for b in builds],
                           "graph_launches": build_graphs,
                           "work": {"join_pairs": b_pairs, "join_list_entries": b_lists, "iterations": b_iters},
+                          # per NN-descent iteration: device ms, join pairs, list entries, locked insert
+                          # attempts and inserts that landed (the median build)
+                          "per_iteration": [[round(r["ms"], 3), r["pairs"], r["list_entries"], r["insert_attempts"],
+                                             r["inserts_landed"]] for r in b_periter],
+                          "per_iteration_fields": ["ms", "pairs", "list_entries", "insert_attempts",
+                                                   "inserts_landed"],
                           "roofline": {"bound": "hbm", "algorithmic_bytes": int(build_bytes),
                                        "achieved": build_bytes / (build_ms / 1000) / 1e9, "peak": hbm,
                                        "unit": "GB/s", "frac": build_bytes / (build_ms / 1000) / 1e9 / hbm,

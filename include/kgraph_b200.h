@@ -318,6 +318,19 @@ int kg_last_build_graphs(kg_ctx *ctx, unsigned *graph_launches);
  * dataset rows the joins read) and the iterations run.  Any pointer may be
  * NULL. */
 int kg_last_build_work(kg_ctx *ctx, uint64_t *pairs, uint64_t *list_entries, unsigned *iterations);
+/* The same per NN-descent iteration of the last kg_build (the reference's
+ * per-iteration log line, kgraph.cpp:952-962, has no counterpart for these):
+ * join pairs, join list entries, locked insert attempts (offers that passed the
+ * unlocked radius test, kgraph.cpp:724), inserts that entered a list (not a
+ * duplicate), the iteration's device milliseconds (its launches: the previous
+ * iteration's update, the join, the statistics) and whether its join ran on
+ * the tensor cores.  Fills min(cap, iterations) entries; *n = iterations. */
+typedef struct {
+    unsigned long long pairs, list_entries, insert_attempts, inserts_landed;
+    float ms;
+    unsigned tensor_core;
+} kg_build_iteration;
+int kg_last_build_iterations(kg_ctx *ctx, kg_build_iteration *out, unsigned cap, unsigned *n);
 /* Work of the last kg_search_batch: distance evaluations (seeds included;
  * the sum of SearchInfo.cost * N plus the seeds) and adjacency entries read. */
 int kg_last_search_work(kg_ctx *ctx, uint64_t *evaluations, uint64_t *adjacency_reads);

@@ -24,6 +24,7 @@ SYMBOLS = [
     "kg_set_join_precision", "kg_last_join_stats", "kg_last_build_graphs", "kg_search_autotune",
     "kg_set_search_tuning", "kg_get_search_tuning", "kg_set_search_precision", "kg_last_search_filter",
     "kg_filter_bounds", "kg_router_search", "kg_tc_gemm_check", "kg_tc_assign_check", "kg_last_build_work",
+    "kg_last_build_iterations",
 ]
 
 JOIN = {"auto": 0, "fp32": 1, "bf16": 2, "bf16_always": 3}
@@ -71,6 +72,11 @@ class FilterStats(C.Structure):
 
 
 SEARCH_PRECISION = {"fp32": 0, "bf16": 1, "fp8": 2}
+
+
+class BuildIteration(C.Structure):
+    _fields_ = [("pairs", C.c_ulonglong), ("list_entries", C.c_ulonglong), ("insert_attempts", C.c_ulonglong),
+                ("inserts_landed", C.c_ulonglong), ("ms", C.c_float), ("tensor_core", C.c_uint)]
 
 
 class SearchParams(C.Structure):
@@ -128,6 +134,7 @@ def lib():
                                        vp, C.c_int, C.c_float, vp, C.c_int]
         L.kg_tc_assign_check.argtypes = [vp, vp, C.c_int, C.c_int, vp, C.c_int, vp, vp, vp]
         L.kg_last_build_work.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint)]
+        L.kg_last_build_iterations.argtypes = [vp, C.POINTER(BuildIteration), C.c_uint, C.POINTER(C.c_uint)]
         L.kg_index_params_default.argtypes = [C.POINTER(IndexParams)]
         L.kg_search_params_default.argtypes = [C.POINTER(SearchParams)]
         _lib = L
@@ -333,6 +340,14 @@ class Context:
         p, e, it = C.c_uint64(), C.c_uint64(), C.c_uint()
         self._check(self.L.kg_last_build_work(self.h, C.byref(p), C.byref(e), C.byref(it)))
         return p.value, e.value, it.value
+
+    def build_iterations(self):
+        """kg_last_build_iterations: per-iteration counters and device milliseconds of the last build."""
+        n = C.c_uint()
+        self._check(self.L.kg_last_build_iterations(self.h, None, 0, C.byref(n)))
+        arr = (BuildIteration * max(1, n.value))()
+        self._check(self.L.kg_last_build_iterations(self.h, arr, n.value, C.byref(n)))
+        return [{f: getattr(arr[i], f) for f, _ in BuildIteration._fields_} for i in range(n.value)]
 
     def search_work(self):
         ev, adj = C.c_uint64(), C.c_uint64()

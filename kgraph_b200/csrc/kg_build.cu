@@ -214,6 +214,7 @@ __global__ void __launch_bounds__(256) join_kernel(BuildState s) {
     const int g = lane >> 2, t = lane & 3;
     const uint32_t N = s.D.n;
     unsigned long long comps = 0;
+    InsertTally tally;
     for (;;) {
         uint32_t n = 0;
         if (lane == 0) n = atomicAdd(s.work, 1u);
@@ -238,9 +239,9 @@ __global__ void __launch_bounds__(256) join_kernel(BuildState s) {
                 const uint32_t xg = __shfl_sync(FULL, x, src), yg = __shfl_sync(FULL, y, src);
                 const float dg = __shfl_sync(FULL, dd, src);
                 uint32_t r = s.Lp;
-                if (nx & (1u << src)) r = locked_insert(s, xg, yg, dg, lane);
+                if (nx & (1u << src)) r = locked_insert(s, xg, yg, dg, lane, tally);
                 if (r < s.K) uu = true;
-                if (ny & (1u << (src + 1))) locked_insert(s, yg, xg, dg, lane);
+                if (ny & (1u << (src + 1))) locked_insert(s, yg, xg, dg, lane, tally);
             }
         };
         for (uint32_t ii = 0; ii < a; ii += 2) {
@@ -273,6 +274,10 @@ __global__ void __launch_bounds__(256) join_kernel(BuildState s) {
         if (lane == 0) s.found[n] = uu ? 1u : 0u;
     }
     if (lane == 0 && comps) atomicAdd(s.n_comps, comps);
+    if (lane == 0 && tally.attempts) {
+        atomicAdd(s.inserts, tally.attempts);
+        atomicAdd(s.inserts + 1, tally.landed);
+    }
 }
 
 // ------------------------------------------------------------------ statistics
@@ -637,7 +642,7 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
     cudaError_t e;
     size_t need[] = {n * s.PS * 4, n * s.PS * 4, n * 4, n * 4, n * 4, n * 4, n * 4, n * 4,
                      n * s.NEWCAP * 4, n * 4, n * s.OLDCAP * 4, n * 4, (n + 1) * 4, (n + 1) * 4,
-                     (n + 1) * 8, (n + 1) * 8, n * L * 4 + 4, n * L * 4 + 4, 64};
+                     (n + 1) * 8, (n + 1) * 8, n * L * 4 + 4, n * L * 4 + 4, 128};
     for (int i = 0; i < 19; ++i)
         if ((e = B[i].reserve(need[i])) != cudaSuccess) return cuda_fail(ctx, e, "alloc build state");
     s.pool_d = B[0].as<float>(); s.pool_i = B[1].as<uint32_t>();
@@ -653,10 +658,12 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
     s.stat = s.n_comps + 1;
     s.work = reinterpret_cast<uint32_t *>(s.n_comps + 4);
     s.iter = s.work + 2;
-    s.list_entries = s.n_comps + 6;   // 64-byte block: n_comps, stat[3], work, iter, list_entries
+    // 128-byte counter block: n_comps, stat[3], work + iter, list_entries, inserts[2]
+    s.list_entries = s.n_comps + 6;
+    s.inserts = s.n_comps + 7;
     s.err = ctx->errw.as<uint32_t>();
     cudaStream_t st = ctx->stream;
-    cudaMemsetAsync(B[18].p, 0, 64, st);
+    cudaMemsetAsync(B[18].p, 0, 128, st);
     if ((e = ctx->tcstat.reserve(sizeof(JoinTcStats))) != cudaSuccess) return cuda_fail(ctx, e, "alloc build state");
     s.tc = ctx->tcstat.as<JoinTcStats>();
     cudaMemsetAsync(s.tc, 0, sizeof(JoinTcStats), st);
@@ -724,6 +731,15 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
     const unsigned long long *hstat = reinterpret_cast<unsigned long long *>(hp.p);
     const float *hout = reinterpret_cast<float *>(hp.p + 64);
     unsigned long long fp32_pairs = 0, hstat_prev = 0;
+    const unsigned long long *hwork = reinterpret_cast<const unsigned long long *>(hp.p + 40);
+    unsigned long long work_prev[3] = {0, 0, 0};
+    ctx->last_build_iters.clear();
+    struct EventPair {   // device time of one iteration's launches
+        cudaEvent_t a = nullptr, b = nullptr;
+        ~EventPair() { if (a) cudaEventDestroy(a); if (b) cudaEventDestroy(b); }
+    } itev;
+    if ((e = cudaEventCreate(&itev.a)) != cudaSuccess || (e = cudaEventCreate(&itev.b)) != cudaSuccess)
+        return cuda_fail(ctx, e, "events");
     double full_frac = 0.0;   // fraction of full pools after the last join
     unsigned tc_iters = 0;
 
@@ -739,6 +755,7 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
         stats_kernel<<<grid_for(ctx, 4), 256, 0, st>>>(s);
         if (C) controls_kernel<<<(C + 127) / 128, 128, 0, st>>>(s, ctrl, ctrl_d, C, ctrl_out);
         cudaMemcpyAsync(hp.p, s.n_comps, 4 * 8, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(hp.p + 40, s.list_entries, 3 * 8, cudaMemcpyDeviceToHost, st);   // lists, inserts[2]
         if (C) cudaMemcpyAsync(hp.p + 64, ctrl_out, (size_t)C * 5 * 4, cudaMemcpyDeviceToHost, st);
         return cudaGetLastError();
     };
@@ -784,6 +801,7 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
     };
     for (uint32_t it = 0; (params->iterations <= 0) || (it < params->iterations); ++it) {
         ++inf.iterations;
+        cudaEventRecord(itev.a, st);
         // The tensor-core filter can only skip pairs against finite radii: while
         // most pools are still filling, every pair passes it and the fused
         // CUDA-core join is the cheaper path.
@@ -823,9 +841,21 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
             if (e != cudaSuccess) return cuda_fail(ctx, e, "iteration graph");
         }
         pending_update = false;
+        cudaEventRecord(itev.b, st);
         if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "join");
         int de = check_device_error(ctx, "build");
         if (de != KG_OK) return de;
+        {
+            kg_build_iteration rec{};
+            rec.pairs = hstat[0] - hstat_prev;
+            rec.list_entries = hwork[0] - work_prev[0];
+            rec.insert_attempts = hwork[1] - work_prev[1];
+            rec.inserts_landed = hwork[2] - work_prev[2];
+            cudaEventElapsedTime(&rec.ms, itev.a, itev.b);
+            rec.tensor_core = tc_now ? 1u : 0u;
+            for (int k = 0; k < 3; ++k) work_prev[k] = hwork[k];
+            ctx->last_build_iters.push_back(rec);
+        }
         // kgraph.cpp:927-963: the per-iteration statistics
         if (!tc_now) fp32_pairs += hstat[0] - hstat_prev;
         hstat_prev = hstat[0];
@@ -921,6 +951,14 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
     ctx->last_build_work[1] = lists;
     ctx->last_build_work[2] = inf.iterations;
     if (info) *info = inf;
+    return KG_OK;
+}
+
+extern "C" int kg_last_build_iterations(kg_ctx *ctx, kg_build_iteration *out, unsigned cap, unsigned *n) {
+    if (!ctx || !n) return KG_E_INVALID;
+    std::lock_guard<std::mutex> guard(ctx->mu);
+    *n = (unsigned)ctx->last_build_iters.size();
+    for (unsigned i = 0; out && i < cap && i < *n; ++i) out[i] = ctx->last_build_iters[i];
     return KG_OK;
 }
 

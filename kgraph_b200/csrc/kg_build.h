@@ -27,6 +27,7 @@ struct BuildState {
     unsigned long long *n_comps;         // join pair counter
     unsigned long long *stat;            // [0] flagged-in-top-K count, [1] sum of M, [2] full pools
     unsigned long long *list_entries;    // join list entries (|new| + |old| summed over nodes and iterations)
+    unsigned long long *inserts;         // [0] locked insert attempts, [1] of those landed (both cumulative)
     uint32_t *err;
     uint32_t *work;                      // dynamic work counter
     uint64_t seed;

@@ -49,6 +49,7 @@ struct kg_ctx {
     float last_build_ms = 0.f, last_search_ms = 0.f, last_router_ms = 0.f;
     unsigned last_build_graph_launches = 0;   // CUDA graph launches of the last build's iterations
     unsigned long long last_build_work[3] = {0, 0, 0};   // join pairs, join list entries, iterations
+    std::vector<kg_build_iteration> last_build_iters;    // per-iteration counters and device time
     unsigned long long last_work[4] = {0, 0, 0, 0};   // evaluations, adjacency reads, filter: approx, skipped
 
     // dataset

@@ -50,12 +50,20 @@ __device__ __forceinline__ uint32_t update_knn_regs(volatile float *pd, volatile
     return i;
 }
 
+// Counts of one warp's inserts: attempts (offers that passed the unlocked
+// radius test and took the lock) and landed (entered the list: not a
+// duplicate), warp-uniform.
+struct InsertTally {
+    unsigned long long attempts = 0, landed = 0;
+};
+
 // Nhood::parallel_try_insert (kgraph.cpp:723-736) by one warp.  Returns the
 // reference's value: pool.size() when the radius test rejects, L+1 for a
 // duplicate, else the insert position.  The lock is taken with an acquire
 // CAS and released with a release store by lane 0; the warp barriers order
 // the other lanes' pool accesses inside that critical section.
-__device__ __forceinline__ uint32_t locked_insert(const BuildState &s, uint32_t x, uint32_t y, float d, int lane) {
+__device__ __forceinline__ uint32_t locked_insert(const BuildState &s, uint32_t x, uint32_t y, float d, int lane,
+                                                  InsertTally &tally) {
     float rad = 0.f;
     uint32_t Lc = 0;
     if (lane == 0) rad = *reinterpret_cast<volatile float *>(s.radius + x);
@@ -83,6 +91,8 @@ __device__ __forceinline__ uint32_t locked_insert(const BuildState &s, uint32_t 
         r = warp_update_knn(pd, pi, (uint32_t *)nullptr, Lc, d, y | FLAG_BIT, 0u, lane);
     }
     __syncwarp();
+    ++tally.attempts;
+    if (r <= Lc) ++tally.landed;
     if (lane == 0 && r <= Lc) {
         if (Lc + 1 < s.Lp) *reinterpret_cast<volatile uint32_t *>(s.nodeL + x) = Lc + 1;
         else *reinterpret_cast<volatile float *>(s.radius + x) = pd[Lc - 1];   // after the shift

@@ -450,6 +450,7 @@ __global__ void __launch_bounds__(256) join_insert_kernel(BuildState s, JoinQueu
     const unsigned long long total = *jq.tail;
     const unsigned long long w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const unsigned long long nw = (gridDim.x * blockDim.x) >> 5;
+    InsertTally tally;
     // one contiguous run of entries per warp: a node's pairs share rows
     const unsigned long long chunk = ((total + nw - 1) / nw + 7) & ~7ull;
     const unsigned long long end = min(total, (w0 + 1) * chunk);
@@ -470,10 +471,14 @@ __global__ void __launch_bounds__(256) join_insert_kernel(BuildState s, JoinQueu
             const uint32_t ng = __shfl_sync(FULL, nn, src);
             const float dg = __shfl_sync(FULL, dd, src);
             uint32_t r = s.Lp;
-            if (nx & (1u << src)) r = locked_insert(s, xg, yg, dg, lane);
+            if (nx & (1u << src)) r = locked_insert(s, xg, yg, dg, lane, tally);
             if (r < s.K && lane == 0) s.found[ng] = 1u;
-            if (ny & (1u << (src + 1))) locked_insert(s, yg, xg, dg, lane);
+            if (ny & (1u << (src + 1))) locked_insert(s, yg, xg, dg, lane, tally);
         }
+    }
+    if (lane == 0 && tally.attempts) {
+        atomicAdd(s.inserts, tally.attempts);
+        atomicAdd(s.inserts + 1, tally.landed);
     }
 }
 
