@@ -169,6 +169,34 @@ int kg_last_search_filter(kg_ctx *ctx, kg_search_filter_stats *out);
 int kg_filter_bounds(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes, const uint32_t *ids,
                      size_t per_query, float *lb, float *dist);
 
+/* Brute-force path of kg_search_batch (every query of a batch with P >= N, or
+ * no graph: SearchOracle::search, kgraph.cpp:231-252; the Python module's
+ * blas=True, python-api.cpp:131-205).  Results are identical in every mode.
+ *   KG_BRUTEFORCE_AUTO    the tensor-core path where it applies (K <= 128,
+ *                         d <= 256, at least 1024 rows), else the CUDA cores;
+ *   KG_BRUTEFORCE_SCAN    one warp per query scans every row in id order on the
+ *                         CUDA cores (the reference's loop);
+ *   KG_BRUTEFORCE_TENSOR  the tensor-core path where it applies: rows and
+ *                         queries centred and rounded to BF16, their products on
+ *                         tcgen05 (FP32 accumulation) give an approximate
+ *                         distance; a rigorous margin of its error selects, per
+ *                         query, every row that can be among the K nearest, and
+ *                         those are evaluated with the canonical FP32 distance.
+ *                         No counterpart in the reference.  Memory: a BF16 copy
+ *                         of the dataset (n * round_up(d, 16) * 2 bytes), built on
+ *                         first use. */
+enum { KG_BRUTEFORCE_AUTO = 0, KG_BRUTEFORCE_SCAN = 1, KG_BRUTEFORCE_TENSOR = 2 };
+int kg_set_bruteforce_mode(kg_ctx *ctx, int mode);
+/* The last brute-force batch: tensor = 1 when it ran on the tensor cores;
+ * candidates = rows evaluated in FP32 over all queries; full_scans = queries
+ * whose candidates exceeded the per-query capacity (max(1024, 8 K)) and were
+ * scanned in full instead. */
+typedef struct {
+    int tensor;
+    unsigned long long candidates, full_scans;
+} kg_bruteforce_stats;
+int kg_last_bruteforce_stats(kg_ctx *ctx, kg_bruteforce_stats *out);
+
 /* KGraphImpl::reverse (kgraph.cpp:667-702) on the current graph. */
 int kg_reverse(kg_ctx *ctx, int rev_k);
 /* KGraph::prune (kgraph.h:180; kgraph.cpp:584-665) on the current graph. */

@@ -21,7 +21,7 @@ LIB = os.path.join(PKG, "libkgraph_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 CUDA_SOURCES = ["kg_ctx.cu", "kg_search.cu", "kg_build.cu", "kg_graph.cu", "kg_noalloc.cu", "kg_router.cu",
-                "kg_join_tc.cu", "kg_precision.cu", "kg_gemm.cu", "kg_checks.cu"]
+                "kg_join_tc.cu", "kg_precision.cu", "kg_gemm.cu", "kg_checks.cu", "kg_bruteforce.cu"]
 CXX_SOURCES = ["kgraph_api.cpp"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",

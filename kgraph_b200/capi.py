@@ -24,7 +24,7 @@ SYMBOLS = [
     "kg_set_join_precision", "kg_last_join_stats", "kg_last_build_graphs", "kg_search_autotune",
     "kg_set_search_tuning", "kg_get_search_tuning", "kg_set_search_precision", "kg_last_search_filter",
     "kg_filter_bounds", "kg_router_search", "kg_tc_gemm_check", "kg_tc_assign_check", "kg_last_build_work",
-    "kg_last_build_iterations",
+    "kg_last_build_iterations", "kg_set_bruteforce_mode", "kg_last_bruteforce_stats",
 ]
 
 JOIN = {"auto": 0, "fp32": 1, "bf16": 2, "bf16_always": 3}
@@ -77,6 +77,13 @@ SEARCH_PRECISION = {"fp32": 0, "bf16": 1, "fp8": 2}
 class BuildIteration(C.Structure):
     _fields_ = [("pairs", C.c_ulonglong), ("list_entries", C.c_ulonglong), ("insert_attempts", C.c_ulonglong),
                 ("inserts_landed", C.c_ulonglong), ("ms", C.c_float), ("tensor_core", C.c_uint)]
+
+
+class BruteforceStats(C.Structure):
+    _fields_ = [("tensor", C.c_int), ("candidates", C.c_ulonglong), ("full_scans", C.c_ulonglong)]
+
+
+BRUTEFORCE = {"auto": 0, "scan": 1, "tensor": 2}
 
 
 class SearchParams(C.Structure):
@@ -135,6 +142,8 @@ def lib():
         L.kg_tc_assign_check.argtypes = [vp, vp, C.c_int, C.c_int, vp, C.c_int, vp, vp, vp]
         L.kg_last_build_work.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint)]
         L.kg_last_build_iterations.argtypes = [vp, C.POINTER(BuildIteration), C.c_uint, C.POINTER(C.c_uint)]
+        L.kg_set_bruteforce_mode.argtypes = [vp, C.c_int]
+        L.kg_last_bruteforce_stats.argtypes = [vp, C.POINTER(BruteforceStats)]
         L.kg_index_params_default.argtypes = [C.POINTER(IndexParams)]
         L.kg_search_params_default.argtypes = [C.POINTER(SearchParams)]
         _lib = L
@@ -348,6 +357,15 @@ class Context:
         arr = (BuildIteration * max(1, n.value))()
         self._check(self.L.kg_last_build_iterations(self.h, arr, n.value, C.byref(n)))
         return [{f: getattr(arr[i], f) for f, _ in BuildIteration._fields_} for i in range(n.value)]
+
+    def set_bruteforce_mode(self, mode):
+        """kg_set_bruteforce_mode: 'auto', 'scan' (CUDA cores) or 'tensor'."""
+        self._check(self.L.kg_set_bruteforce_mode(self.h, BRUTEFORCE[mode]))
+
+    def bruteforce_stats(self):
+        st = BruteforceStats()
+        self._check(self.L.kg_last_bruteforce_stats(self.h, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in BruteforceStats._fields_}
 
     def search_work(self):
         ev, adj = C.c_uint64(), C.c_uint64()

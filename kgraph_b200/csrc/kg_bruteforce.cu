@@ -1,0 +1,599 @@
+// Exact brute-force k-NN on the fifth-generation tensor cores:
+// SearchOracle::search (kgraph.cpp:231-252) for a whole batch of queries, the
+// path of every query with P >= N (kgraph.cpp:427-433), of searches without an
+// index (python-api.cpp:303-314) and of the Python module's blas=True
+// (python-api.cpp:131-205, whose OpenBLAS product it replaces).
+//
+// The result must be the reference's bit for bit: the K rows with the smallest
+// canonical FP32 distance (kg_common.cuh), ties by id (the reference scans in
+// id order and inserts after equal distances), distances above epsilon left
+// out.  The tensor cores only choose which rows are worth the canonical FP32
+// evaluation:
+//
+//   1. rows and queries are rounded to BF16 -- centred on the dataset mean
+//      first (euclidean, l2sqr) unless BF16 holds the rows exactly; per row the
+//      exact ||x~||^2 and a rigorous bound e_x >= ||(x - mu) - x~|| are kept
+//      (FP64, rounded outward), per query the same;
+//   2. sweep 1 (tcgen05.mma kind::f16, BF16 x BF16 -> FP32 in TMEM, 128
+//      queries x 128 rows per MMA tile, the query tile resident in shared
+//      memory, row tiles double-buffered so staging overlaps the MMAs): an
+//      approximate distance d~ for every (query, row) and, per query and slice
+//      of rows, the K smallest d~;
+//   3. per query: t = the K-th smallest d~ over all slices, and a rigorous
+//      margin M >= |canonical - d~| for every row (from the BF16 errors, the
+//      FP32 accumulation bound of the products, and the canonical distance's
+//      own rounding bound; dataset-wide maxima of the row terms).  Every row of
+//      the exact top K has canonical <= t + M, hence d~ <= t + 2M;
+//   4. sweep 2: the rows with d~ <= t + 2M are the candidates (appended per
+//      query, at most C);
+//   5. one warp per query evaluates its candidates with the canonical FP32
+//      distance and keeps the K smallest by (distance, id) within epsilon --
+//      the reference's list.  A query with more than C candidates is scanned
+//      in full on the CUDA cores instead (counted in the statistics).
+//
+// All tensor-core waits are bounded: a wait that runs out raises
+// ERR_TC_TIMEOUT, waits (bounded) for the MMA in flight, frees the CTA's TMEM
+// and returns; the host turns the error bit into KG_E_DEVICE.
+#include <algorithm>
+#include <cfloat>
+#include <cstring>
+#include <cuda_bf16.h>
+#include "kg_ctx.h"
+#include "kg_bruteforce.h"
+#include "kg_tc.cuh"
+#include "kg_warp.cuh"
+
+namespace kgb {
+namespace {
+
+constexpr int BF_THREADS = 128;           // 4 warps: warp w reads TMEM lanes 32w.. (its 32 queries)
+constexpr uint32_t BF_M = 128;            // queries per tile (TMEM lanes)
+constexpr uint32_t BF_N = 128;            // rows per tile (TMEM columns per accumulator)
+constexpr long long BF_WAIT_CYCLES = 2000000000ll;
+constexpr float U24 = 5.9604645e-8f;      // 2^-24
+constexpr float U23 = 1.1920929e-7f;      // 2^-23
+
+__device__ __forceinline__ unsigned long long ordered_u64(double v) {
+    unsigned long long u = (unsigned long long)__double_as_longlong(v);
+    return (u & 0x8000000000000000ull) ? ~u : (u | 0x8000000000000000ull);
+}
+
+// Column sums of the dataset in FP64 (the mean for centring).
+__global__ void colsum_kernel(DataView D, double *sum) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= D.d) return;
+    const uint32_t parts = gridDim.y, part = blockIdx.y;
+    const uint32_t chunk = (D.n + parts - 1) / parts;
+    double s = 0.0;
+    for (uint32_t r = part * chunk; r < min(D.n, (part + 1) * chunk); ++r) s += (double)D.X[(size_t)r * D.ld + c];
+    atomicAdd(sum + c, s);
+}
+
+__global__ void mean_kernel(const double *sum, uint32_t d, uint32_t ld, uint32_t n, int centre, float *mu) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < ld) mu[c] = (centre && c < d) ? (float)(sum[c] / (double)n) : 0.f;
+}
+
+// One warp per row: v = bf16(x - mu) (FP32 subtraction, then rounding), the
+// exact ||v||^2, e >= ||(x - mu) - v|| (FP64, rounded up), and the term the
+// sweep needs per row: ||v||^2 (euclidean, l2sqr) or 1 / canonical norm
+// (angular; 0 for a zero row).  Dataset-wide: max ||v||, max e, max canonical
+// norm term, max e / canonical norm and min positive canonical norm (angular).
+__global__ void prep_rows_kernel(DataView D, const float *mu, __nv_bfloat16 *Xb, float4 *meta,
+                                 unsigned long long *ext) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < D.n; row += warps) {
+        const float *x = D.X + (size_t)row * D.ld;
+        double e2 = 0.0, v2 = 0.0;
+        for (uint32_t j = lane; j < D.ld; j += 32) {
+            const float xc = j < D.d ? __fsub_rn(x[j], mu[j]) : 0.f;
+            const __nv_bfloat16 b = __float2bfloat16_rn(xc);
+            Xb[(size_t)row * D.ld + j] = b;
+            const double vb = (double)__bfloat162float(b);
+            const double ex = j < D.d ? ((double)x[j] - (double)mu[j]) - vb : 0.0;
+            e2 += ex * ex;
+            v2 += vb * vb;
+        }
+        for (int o = 16; o; o >>= 1) {
+            e2 += __shfl_xor_sync(FULL, e2, o);
+            v2 += __shfl_xor_sync(FULL, v2, o);
+        }
+        if (lane == 0) {
+            const float e = e2 > 0.0 ? __double2float_ru(sqrt(e2) * (1.0 + 1e-12)) : 0.f;
+            const float nt = D.norms ? D.norms[row] : 0.f;   // canonical norm term (euclidean / angular)
+            float aux;
+            if (D.metric == METRIC_ANGULAR) aux = nt > 0.f ? 1.0f / nt : 0.f;
+            else aux = (float)v2;   // exact: BF16 squares sum exactly in FP64 for d <= 2^20
+            meta[row] = make_float4(aux, e, (float)v2, nt);
+            atomicMax(ext + 0, ordered_u64(sqrt(v2)));
+            atomicMax(ext + 1, ordered_u64((double)e));
+            atomicMax(ext + 2, ordered_u64((double)nt));
+            if (D.metric == METRIC_ANGULAR && nt > 0.f) {
+                atomicMax(ext + 3, ordered_u64((double)e / (double)nt));
+                atomicMin(ext + 4, ordered_u64((double)nt));
+            }
+        }
+    }
+}
+
+// One warp per query: the same centring and rounding, and the canonical norm
+// term of the query (the search kernel's computation: python-api.cpp:98-101).
+__global__ void prep_queries_kernel(DataView D, const float *mu, const float *Q, uint32_t q_ld, uint32_t nq,
+                                    __nv_bfloat16 *Qb, float4 *qmeta) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t qi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; qi < nq; qi += warps) {
+        const float *q = Q + (size_t)qi * q_ld;
+        double e2 = 0.0, v2 = 0.0;
+        for (uint32_t j = lane; j < D.ld; j += 32) {
+            const float xc = j < D.d ? __fsub_rn(q[j], mu[j]) : 0.f;
+            const __nv_bfloat16 b = __float2bfloat16_rn(xc);
+            Qb[(size_t)qi * D.ld + j] = b;
+            const double vb = (double)__bfloat162float(b);
+            const double ex = j < D.d ? ((double)q[j] - (double)mu[j]) - vb : 0.0;
+            e2 += ex * ex;
+            v2 += vb * vb;
+        }
+        for (int o = 16; o; o >>= 1) {
+            e2 += __shfl_xor_sync(FULL, e2, o);
+            v2 += __shfl_xor_sync(FULL, v2, o);
+        }
+        float qn = 0.f;
+        if (D.metric != METRIC_L2SQR) {
+            // the canonical order needs the query's padding columns at zero: read through a masked copy
+            float n2;
+            {
+                float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+                const int t = lane & 3;
+                const uint32_t chunks = D.d >> 4;
+                for (uint32_t c = 0; c < chunks; ++c) lane_acc(acc, ld4(q + 16 * c + 4 * t), ld4(q + 16 * c + 4 * t), METRIC_EUCLIDEAN);
+                n2 = group4_reduce(acc, FULL);
+                uint32_t i = chunks << 4;
+                if (D.d - i >= 8)
+                    for (uint32_t e = i + 8; i < e; ++i) n2 = __fadd_rn(n2, __fmul_rn(q[i], q[i]));
+                for (; i < D.d; ++i) n2 = __fmaf_rn(q[i], q[i], n2);
+            }
+            qn = norm_term(n2, D.metric);
+        }
+        if (lane == 0) {
+            const float e = e2 > 0.0 ? __double2float_ru(sqrt(e2) * (1.0 + 1e-12)) : 0.f;
+            qmeta[qi] = make_float4((float)v2, e, qn, 0.f);
+        }
+    }
+}
+
+struct SweepArgs {
+    const __nv_bfloat16 *Xb, *Qb;
+    const float4 *meta, *qmeta;
+    uint32_t n, ld, nq, K, slices, slice_rows, metric, cap;
+    float *topk;            // mode 0 out: [nq][slices][K] smallest d~ per slice (ascending, +inf padded)
+    const float *thresh;    // mode 1 in: per query t + 2M
+    uint32_t *cand, *cand_n;   // mode 1 out: [nq][cap] candidate ids, per-query count (may exceed cap)
+    uint32_t *err;
+};
+
+// Stages `rows` rows starting at r0 of a BF16 matrix (row stride ld) into a
+// K-major core-matrix tile of ld columns; rows past `rows` are zero.
+__device__ __forceinline__ void stage_bf16_tile(uint8_t *tile, const __nv_bfloat16 *src, uint32_t ld, uint32_t r0,
+                                                uint32_t rows, int tid) {
+    const uint32_t k8n = ld >> 3;
+    for (uint32_t e = tid; e < BF_N * k8n; e += BF_THREADS) {
+        const uint32_t r = e / k8n, k8 = e % k8n;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (r < rows) v = *reinterpret_cast<const uint4 *>(src + (size_t)(r0 + r) * ld + 8 * k8);
+        *reinterpret_cast<uint4 *>(tile + tc::kmajor_off(r, 8 * k8, ld)) = v;
+    }
+}
+
+// d~ of a (query, row) pair from its product g: euclidean and l2sqr from the
+// centred norms, angular from the uncentred product and the inverse norms.
+__device__ __forceinline__ float approx_d(uint32_t metric, float g, float qa, float qb, float ra) {
+    if (metric == METRIC_ANGULAR) return -(g * qb) * ra;          // qb = 1 / n_q, ra = 1 / n_x
+    const float a = __fadd_rn(qa, ra) - 2.0f * g;                 // ||q~ - x~||^2 from the expansion
+    return metric == METRIC_L2SQR ? a : 0.5f * a;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(BF_THREADS, 1) bf_sweep_kernel(SweepArgs a) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ uint32_t tmem_base;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t q0 = blockIdx.x * BF_M;
+    const uint32_t slice = blockIdx.y;
+    const uint32_t rbeg = slice * a.slice_rows, rend = min(a.n, rbeg + a.slice_rows);
+    const size_t tile_bytes = (size_t)BF_N * a.ld * 2;
+    uint8_t *sQ = smem;   // row tile b at smem + (1 + b) * tile_bytes
+    float *rterm = reinterpret_cast<float *>(smem + 3 * tile_bytes);   // [2][BF_N] per-row term
+    float *heap = rterm + 2 * BF_N;                                     // MODE 0: [BF_M][K] sorted ascending
+    if (warp == 0) tc::tmem_alloc(&tmem_base, 2 * BF_N);
+    if (tid == 0) { tc::mbar_init(&mbar[0], 1); tc::mbar_init(&mbar[1], 1); }
+    // the query tile, and this thread's query terms
+    stage_bf16_tile(sQ, a.Qb, a.ld, q0, min(BF_M, a.nq - q0), tid);
+    const uint32_t myq = q0 + 32 * warp + lane;
+    const bool qok = myq < a.nq;
+    float qa = 0.f, qb = 0.f;
+    if (qok) {
+        const float4 qm = a.qmeta[myq];
+        qa = qm.x;                                  // ||q~||^2
+        qb = qm.z > 0.f ? 1.0f / qm.z : 0.f;        // angular: 1 / n_q
+    }
+    float kth = FLT_MAX;        // MODE 0: the K-th smallest so far; MODE 1: the threshold
+    uint32_t have = 0;
+    float *mine = heap + (size_t)(32 * warp + lane) * a.K;
+    if (MODE == 1 && qok) kth = a.thresh[myq];
+    const uint32_t ntiles = rend > rbeg ? (rend - rbeg + BF_N - 1) / BF_N : 0;
+    auto stage_rows = [&](uint32_t t) {
+        const uint32_t r0 = rbeg + t * BF_N;
+        const uint32_t rows = min(BF_N, rend - r0);
+        stage_bf16_tile(smem + (1 + (t & 1)) * tile_bytes, a.Xb, a.ld, r0, rows, tid);
+        for (uint32_t r = tid; r < BF_N; r += BF_THREADS) rterm[(t & 1) * BF_N + r] = r < rows ? a.meta[r0 + r].x : 0.f;
+    };
+    if (ntiles) stage_rows(0);
+    tc::fence_async_shared();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_base;
+    const uint32_t idesc = tc::idesc_bf16_f32(BF_M, BF_N);
+    auto issue = [&](uint32_t t) {
+        tc::fence_after_sync();
+        const uint32_t aa = tc::smem_addr(sQ), ba = tc::smem_addr(smem + (1 + (t & 1)) * tile_bytes);
+        for (uint32_t kk = 0; kk < a.ld / 16; ++kk)
+            tc::mma_bf16(tmem + (t & 1) * BF_N, tc::smem_desc(aa + kk * 256, 128, a.ld * 16),
+                         tc::smem_desc(ba + kk * 256, 128, a.ld * 16), idesc, kk > 0 ? 1u : 0u);
+        tc::mma_commit(&mbar[t & 1]);
+    };
+    if (ntiles && tid == 0) issue(0);
+    uint32_t phases = 0u;   // bit b: the parity barrier b waits for next
+    bool ok = true;
+    uint32_t failed = 0;   // the tile whose completion wait ran out
+    for (uint32_t t = 0; t < ntiles; ++t) {
+        if (t + 1 < ntiles) stage_rows(t + 1);   // its buffer was last read by MMA t-1 (completed)
+        tc::fence_async_shared();
+        tc::fence_before_sync();
+        __syncthreads();
+        const bool done = tc::mbar_wait(&mbar[t & 1], (phases >> (t & 1)) & 1u, BF_WAIT_CYCLES);
+        ok = !__syncthreads_or(!done);
+        if (!ok) { failed = t; break; }
+        phases ^= 1u << (t & 1);
+        tc::fence_after_sync();
+        if (t + 1 < ntiles && tid == 0) issue(t + 1);   // runs while this tile's epilogue does
+        // epilogue: this thread's query against the tile's 128 rows
+        const uint32_t r0 = rbeg + t * BF_N;
+        const uint32_t rows = min(BF_N, rend - r0);
+        const float *rt = rterm + (t & 1) * BF_N;
+        for (uint32_t part = 0; part < BF_N / 32; ++part) {
+            if (32 * part >= rows) break;   // uniform over the CTA
+            float v[32];
+            tc::tmem_ld32(tmem + (t & 1) * BF_N + ((uint32_t)(32 * warp) << 16) + 32 * part, v);
+            if (!qok) continue;
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+                const uint32_t col = 32 * part + c;
+                if (col >= rows) continue;
+                const float dt = approx_d(a.metric, v[c], qa, qb, rt[col]);
+                if (MODE == 0) {
+                    if (dt < kth || have < a.K) {   // sorted insert into this query's K smallest
+                        uint32_t p = have < a.K ? have++ : a.K - 1;
+                        while (p > 0 && mine[p - 1] > dt) { mine[p] = mine[p - 1]; --p; }
+                        mine[p] = dt;
+                        if (have == a.K) kth = mine[a.K - 1];
+                    }
+                } else if (dt <= kth) {
+                    const uint32_t pos = atomicAdd(a.cand_n + myq, 1u);
+                    if (pos < a.cap) a.cand[(size_t)myq * a.cap + pos] = r0 + col;
+                }
+            }
+        }
+        tc::fence_before_sync();
+        __syncthreads();   // the accumulator and the row buffer of tile t are reused by tile t+2
+        tc::fence_after_sync();
+    }
+    if (!ok) {
+        if (tid == 0) raise_error(a.err, ERR_TC_TIMEOUT);
+        // the MMA that was waited for may still run (no later one was issued): one more bounded
+        // wait before the TMEM goes
+        tc::mbar_wait(&mbar[failed & 1], (phases >> (failed & 1)) & 1u, BF_WAIT_CYCLES);
+    } else if (MODE == 0 && qok) {
+        float *out = a.topk + ((size_t)myq * a.slices + slice) * a.K;
+        for (uint32_t k = 0; k < a.K; ++k) out[k] = k < have ? mine[k] : FLT_MAX;
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_free(tmem, 2 * BF_N);
+}
+
+struct Extents {   // dataset-wide row terms (prep_rows_kernel)
+    float vmax, emax, ntmax, relmax, ntmin;
+};
+
+// Per query: t = K-th smallest d~ over the slices, margin M, threshold t + 2M.
+__global__ void bf_threshold_kernel(const float *topk, const float4 *qmeta, uint32_t nq, uint32_t slices, uint32_t K,
+                                    uint32_t d, uint32_t metric, Extents ex, float *thresh) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t qi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (qi >= nq) return;
+    // K-way merge of the sorted slice lists: lane s holds the head of slice s (slices <= 32)
+    const float *base = topk + (size_t)qi * slices * K;
+    uint32_t pos = 0;
+    float t = FLT_MAX;
+    for (uint32_t k = 0; k < K; ++k) {
+        const float head = ((uint32_t)lane < slices && pos < K) ? base[(size_t)lane * K + pos] : FLT_MAX;
+        float m = head;
+        for (int o = 16; o; o >>= 1) m = fminf(m, __shfl_xor_sync(FULL, m, o));
+        const unsigned who = __ballot_sync(FULL, head == m);
+        if (lane == __ffs(who) - 1) ++pos;
+        t = m;
+    }
+    if (lane != 0) return;
+    const float4 qm = qmeta[qi];
+    const float qv = sqrtf(qm.x) * (1.f + 4.f * U24);     // ||q~||, rounded up
+    const float eq = qm.y, qn = qm.z;
+    const float gc = (float)(d / 16 + 24) * U24 * 1.01f;   // canonical distance's relative rounding bound
+    float M;
+    if (metric == METRIC_ANGULAR) {
+        if (!(qn > 0.f) || !(ex.ntmin > 0.f)) { thresh[qi] = FLT_MAX; return; }
+        const float rq = eq / qn, rx = ex.relmax;
+        const float core = (1.f + 2.f * gc) * (gc + (float)d * U23 * (1.f + rq) * (1.f + rx) + rq * (1.f + rx) + rx);
+        M = 1.25f * (core + (1.f + rq) * (1.f + rx) * (FLT_EPSILON / (qn * ex.ntmin) + 8.f * U23)) + 1e-30f;
+    } else {
+        const float X = ex.vmax, e = eq + ex.emax;
+        const float s = qv + X;
+        const float EA = (2.f * (float)d + 4.f) * U23 * s * s;   // |A~ - ||q~ - x~||^2|
+        const float E2 = EA + 2.f * e * s + e * e;                 // |A~ - ||q - x||^2|
+        if (metric == METRIC_L2SQR) M = 1.25f * (E2 + gc * (s + e) * (s + e));
+        else M = 1.25f * (0.5f * E2 + 2.5f * gc * (qn + ex.ntmax));
+        M += 1e-30f;
+    }
+    thresh[qi] = (t >= FLT_MAX) ? FLT_MAX : __fadd_ru(t, 2.f * M * (1.f + 1e-6f));
+}
+
+// Orderable 64-bit key: (distance, id) ascending; -0 and +0 compare equal, as in the reference.
+__device__ __forceinline__ unsigned long long dist_key(float d, uint32_t id) {
+    uint32_t u = __float_as_uint(d == 0.f ? 0.f : d);
+    u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+    return ((unsigned long long)u << 32) | id;
+}
+__device__ __forceinline__ float key_dist(unsigned long long k) {
+    uint32_t u = (uint32_t)(k >> 32);
+    u = (u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u;
+    return __uint_as_float(u);
+}
+
+// One warp per query: canonical FP32 distances of the candidates, then the K
+// smallest by (distance, id) within epsilon; a query whose candidates
+// overflowed is scanned in full.
+__global__ void __launch_bounds__(256) bf_recheck_kernel(DataView D, const float *Q, uint32_t q_ld, uint32_t nq,
+                                                         uint32_t K, float epsilon, const uint32_t *cand,
+                                                         const uint32_t *cand_n, uint32_t cap, uint32_t *out_ids,
+                                                         float *out_d, uint32_t *out_cnt, float *out_cost,
+                                                         uint32_t out_ld, unsigned long long *stats,
+                                                         unsigned long long *work) {
+    extern __shared__ __align__(16) unsigned char rsm[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t qi = blockIdx.x * (blockDim.x >> 5) + w;
+    if (qi >= nq) return;   // whole warps
+    float *q = reinterpret_cast<float *>(rsm) + (size_t)w * D.ld;
+    unsigned long long *keys = reinterpret_cast<unsigned long long *>(rsm + (size_t)(blockDim.x >> 5) * D.ld * 4) +
+                               (size_t)w * cap;
+    for (uint32_t x = lane; x < D.ld; x += 32) q[x] = x < D.d ? Q[(size_t)qi * q_ld + x] : 0.f;
+    __syncwarp();
+    float qn = 0.f;
+    if (D.metric != METRIC_L2SQR) qn = norm_term(group4_raw(q, q, D.d, METRIC_EUCLIDEAN, lane & 3, FULL), D.metric);
+    const uint32_t nc = cand_n[qi];
+    const bool full = nc > cap;
+    const uint32_t total = full ? D.n : nc;
+    const int g = lane >> 2, t = lane & 3;
+    // the K smallest keys so far live in keys[0..have) when scanning in full; else all candidates' keys
+    uint32_t nkeys = 0;
+    unsigned long long worst = ~0ull;   // full scan: the K-th smallest key so far
+    for (uint32_t base = 0; base < total; base += 8) {
+        const uint32_t i = base + g;
+        const uint32_t id = i < total ? (full ? i : cand[(size_t)qi * cap + i]) : 0u;
+        const float dd = query_dist(D, q, qn, id, t, FULL);
+        const bool keep = i < total && t == 0 && !(dd > epsilon);
+        const unsigned long long key = dist_key(dd, id);
+        unsigned km = __ballot_sync(FULL, keep && (!full || key < worst));
+        while (km) {
+            const int src = __ffs(km) - 1;
+            km &= km - 1;
+            const unsigned long long kk = __shfl_sync(FULL, key, src);
+            if (!full) {
+                if (lane == 0) keys[nkeys] = kk;
+                ++nkeys;
+            } else if (kk < worst) {   // keep the K smallest keys, unsorted; evict the largest
+                if (nkeys < K) {
+                    if (lane == 0) keys[nkeys] = kk;
+                    ++nkeys;
+                } else {
+                    // replace the largest key
+                    unsigned long long mx = 0;
+                    uint32_t at = 0;
+                    for (uint32_t j = lane; j < nkeys; j += 32)
+                        if (keys[j] >= mx) { mx = keys[j]; at = j; }
+                    for (int o = 16; o; o >>= 1) {
+                        const unsigned long long om = __shfl_xor_sync(FULL, mx, o);
+                        const uint32_t oa = __shfl_xor_sync(FULL, at, o);
+                        if (om > mx || (om == mx && oa > at)) { mx = om; at = oa; }
+                    }
+                    __syncwarp();
+                    if (lane == 0) keys[at] = kk;
+                }
+                __syncwarp();
+                if (nkeys == K) {   // the new K-th smallest
+                    unsigned long long mx = 0;
+                    for (uint32_t j = lane; j < nkeys; j += 32) mx = max(mx, keys[j]);
+                    for (int o = 16; o; o >>= 1) mx = max(mx, __shfl_xor_sync(FULL, mx, o));
+                    worst = mx;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    __syncwarp();
+    // K rounds of the warp's smallest remaining key
+    const uint32_t cnt = min(K, nkeys);
+    uint32_t *oi = out_ids + (size_t)qi * out_ld;
+    float *od = out_d ? out_d + (size_t)qi * out_ld : nullptr;
+    for (uint32_t k = 0; k < cnt; ++k) {
+        unsigned long long mn = ~0ull;
+        uint32_t at = 0;
+        for (uint32_t j = lane; j < nkeys; j += 32)
+            if (keys[j] < mn) { mn = keys[j]; at = j; }
+        for (int o = 16; o; o >>= 1) {
+            const unsigned long long om = __shfl_xor_sync(FULL, mn, o);
+            const uint32_t oa = __shfl_xor_sync(FULL, at, o);
+            if (om < mn) { mn = om; at = oa; }
+        }
+        if (lane == 0) {
+            oi[k] = (uint32_t)(mn & 0xFFFFFFFFu);
+            if (od) od[k] = key_dist(mn);
+            keys[at] = ~0ull;
+        }
+        __syncwarp();
+    }
+    if (lane == 0) {
+        out_cnt[qi] = cnt;
+        if (out_cost) out_cost[qi] = 1.0f;   // kgraph.cpp:428-431
+        atomicAdd(stats + 0, (unsigned long long)(full ? 0u : nc));
+        if (full) atomicAdd(stats + 1, 1ull);
+        if (work) atomicAdd(work, (unsigned long long)total);
+    }
+}
+
+}  // namespace
+
+bool bruteforce_tc_supported(const kg_ctx *ctx, uint32_t K) {
+    if (K == 0 || K > BF_MAX_K || ctx->ld > 256) return false;
+    return bruteforce_tc_smem(ctx->ld, K) <= 200 * 1024;
+}
+
+// Dynamic shared memory of a sweep CTA: the query tile, two row tiles, the
+// rows' terms and (sweep 1) each query's K smallest.  At least 100 KB, so at
+// most two CTAs (2 x 256 TMEM columns) share an SM.
+size_t bruteforce_tc_smem(uint32_t ld, uint32_t K) {
+    const size_t b = 3ull * BF_N * ld * 2 + 2ull * BF_N * 4 + (size_t)BF_M * K * 4;
+    return std::max<size_t>(b, 100 * 1024);
+}
+
+// Rows of the dataset prepared for the sweeps (once per dataset version).
+// First uncentred: a dataset whose values BF16 holds exactly (small integers,
+// as in the benchmark's mixtures) keeps e_x = 0 and needs no centring.  Any
+// other euclidean / l2sqr dataset is prepared again centred on its mean, which
+// makes the BF16 error scale with the spread of the data instead of its offset.
+int bruteforce_prepare(kg_ctx *ctx) {
+    if (ctx->bf_data_version == ctx->data_version) return KG_OK;
+    const uint32_t n = ctx->n, ld = ctx->ld;
+    cudaError_t e;
+    if ((e = ctx->bf_rows.reserve((size_t)n * ld * 2)) != cudaSuccess ||
+        (e = ctx->bf_meta.reserve((size_t)n * sizeof(float4) + 16)) != cudaSuccess ||
+        (e = ctx->bf_aux.reserve(ld * 8 + ld * 4 + 64)) != cudaSuccess)
+        return cuda_fail(ctx, e, "alloc brute-force rows");
+    cudaStream_t st = ctx->stream;
+    double *sum = ctx->bf_aux.as<double>();
+    float *mu = reinterpret_cast<float *>(sum + ld);
+    unsigned long long *ext = reinterpret_cast<unsigned long long *>(mu + ld);
+    const DataView D{ctx->X.as<float>(), ctx->norms.as<float>(), n, ctx->d, ld, ctx->metric};
+    auto dec = [](unsigned long long o) {
+        unsigned long long u = (o & 0x8000000000000000ull) ? (o & ~0x8000000000000000ull) : ~o;
+        double v;
+        std::memcpy(&v, &u, 8);
+        return v;
+    };
+    unsigned long long h[5];
+    for (int centre = 0; centre < 2; ++centre) {
+        if (centre) {
+            cudaMemsetAsync(sum, 0, ld * 8, st);
+            dim3 grid((ctx->d + 127) / 128, std::min<uint32_t>(1024, (n + 255) / 256));
+            colsum_kernel<<<grid, 128, 0, st>>>(D, sum);
+        }
+        mean_kernel<<<(ld + 127) / 128, 128, 0, st>>>(sum, ctx->d, ld, n, centre, mu);
+        const unsigned long long init[5] = {0, 0, 0, 0, ~0ull};
+        cudaMemcpyAsync(ext, init, sizeof(init), cudaMemcpyHostToDevice, st);
+        prep_rows_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(D, mu, ctx->bf_rows.as<__nv_bfloat16>(),
+                                                           ctx->bf_meta.as<float4>(), ext);
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "brute-force prep");
+        cudaMemcpyAsync(h, ext, sizeof(h), cudaMemcpyDeviceToHost, st);
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "brute-force prep");
+        if (ctx->metric == METRIC_ANGULAR || dec(h[1]) == 0.0) break;   // uncentred: exact, or angular
+    }
+    // dataset maxima, rounded up (the minimum rounded down)
+    ctx->bf_ext[0] = (float)(dec(h[0]) * (1 + 1e-6));
+    ctx->bf_ext[1] = (float)(dec(h[1]) * (1 + 1e-6));
+    ctx->bf_ext[2] = (float)(dec(h[2]) * (1 + 1e-6));
+    ctx->bf_ext[3] = h[3] ? (float)(dec(h[3]) * (1 + 1e-6)) : 0.f;
+    ctx->bf_ext[4] = h[4] != ~0ull ? (float)(dec(h[4]) * (1 - 1e-6)) : 0.f;
+    ctx->bf_data_version = ctx->data_version;
+    return KG_OK;
+}
+
+int bruteforce_tc(kg_ctx *ctx, const float *Q, uint32_t q_ld, uint32_t nq, uint32_t K, float epsilon, uint32_t *out_ids,
+                  float *out_d, uint32_t *out_cnt, float *out_cost, uint32_t out_ld, unsigned long long *work) {
+    int r = bruteforce_prepare(ctx);
+    if (r != KG_OK) return r;
+    const uint32_t n = ctx->n, ld = ctx->ld;
+    cudaStream_t st = ctx->stream;
+    const uint32_t qtiles = (nq + BF_M - 1) / BF_M;
+    uint32_t slices = std::max<uint32_t>(1, (2 * (uint32_t)ctx->num_sms + qtiles - 1) / qtiles);
+    slices = std::min<uint32_t>(slices, 32);
+    slices = std::min<uint32_t>(slices, std::max<uint32_t>(1, (n + BF_N - 1) / BF_N));
+    const uint32_t slice_rows = ((n + slices - 1) / slices + BF_N - 1) / BF_N * BF_N;
+    slices = (n + slice_rows - 1) / slice_rows;
+    const uint32_t cap = std::max<uint32_t>(1024, 8 * K);
+    cudaError_t e;
+    const size_t need = (size_t)nq * ld * 2 + (size_t)nq * 16 + (size_t)nq * slices * K * 4 + (size_t)nq * 4 +
+                        (size_t)nq * cap * 4 + (size_t)nq * 4 + 64 + 6 * 256;
+    if ((e = ctx->bf_work.reserve(need)) != cudaSuccess) return cuda_fail(ctx, e, "alloc brute force");
+    char *p = ctx->bf_work.as<char>();
+    auto carve = [&](size_t bytes) { char *q = p; p += (bytes + 255) / 256 * 256; return q; };
+    __nv_bfloat16 *Qb = reinterpret_cast<__nv_bfloat16 *>(carve((size_t)nq * ld * 2));
+    float4 *qmeta = reinterpret_cast<float4 *>(carve((size_t)nq * 16));
+    float *topk = reinterpret_cast<float *>(carve((size_t)nq * slices * K * 4));
+    float *thresh = reinterpret_cast<float *>(carve((size_t)nq * 4));
+    uint32_t *cand = reinterpret_cast<uint32_t *>(carve((size_t)nq * cap * 4));
+    uint32_t *cand_n = reinterpret_cast<uint32_t *>(carve((size_t)nq * 4));
+    unsigned long long *stats = reinterpret_cast<unsigned long long *>(carve(64));
+    cudaMemsetAsync(cand_n, 0, (size_t)nq * 4, st);
+    cudaMemsetAsync(stats, 0, 64, st);
+    const DataView D{ctx->X.as<float>(), ctx->norms.as<float>(), n, ctx->d, ld, ctx->metric};
+    const float *mu = reinterpret_cast<const float *>(ctx->bf_aux.as<double>() + ld);
+    prep_queries_kernel<<<std::max<uint32_t>(1, std::min<uint32_t>((nq + 7) / 8, ctx->num_sms * 8)), 256, 0, st>>>(
+        D, mu, Q, q_ld, nq, Qb, qmeta);
+    SweepArgs a{};
+    a.Xb = ctx->bf_rows.as<__nv_bfloat16>();
+    a.Qb = Qb;
+    a.meta = ctx->bf_meta.as<float4>();
+    a.qmeta = qmeta;
+    a.n = n; a.ld = ld; a.nq = nq; a.K = K; a.slices = slices; a.slice_rows = slice_rows; a.metric = ctx->metric;
+    a.cap = cap;
+    a.topk = topk;
+    a.thresh = thresh;
+    a.cand = cand;
+    a.cand_n = cand_n;
+    a.err = ctx->errw.as<uint32_t>();
+    const size_t smem0 = bruteforce_tc_smem(ld, K), smem1 = bruteforce_tc_smem(ld, 0);
+    if ((e = cudaFuncSetAttribute(bf_sweep_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem0)) !=
+            cudaSuccess ||
+        (e = cudaFuncSetAttribute(bf_sweep_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1)) !=
+            cudaSuccess)
+        return cuda_fail(ctx, e, "brute-force sweep attributes");
+    const dim3 grid(qtiles, slices);
+    bf_sweep_kernel<0><<<grid, BF_THREADS, smem0, st>>>(a);
+    const Extents ex{ctx->bf_ext[0], ctx->bf_ext[1], ctx->bf_ext[2], ctx->bf_ext[3], ctx->bf_ext[4]};
+    bf_threshold_kernel<<<(nq + 7) / 8, 256, 0, st>>>(topk, qmeta, nq, slices, K, ctx->d, ctx->metric, ex, thresh);
+    bf_sweep_kernel<1><<<grid, BF_THREADS, smem1, st>>>(a);
+    const uint32_t wpb = 4;
+    const size_t rsmem = (size_t)wpb * (ld * 4 + (size_t)cap * 8);
+    if ((e = cudaFuncSetAttribute(bf_recheck_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem)) !=
+        cudaSuccess)
+        return cuda_fail(ctx, e, "brute-force recheck attributes");
+    bf_recheck_kernel<<<(nq + wpb - 1) / wpb, wpb * 32, rsmem, st>>>(D, Q, q_ld, nq, K, epsilon, cand, cand_n, cap,
+                                                                     out_ids, out_d, out_cnt, out_cost, out_ld, stats, work);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "brute-force launch");
+    ctx->bf_stats_dev = stats;   // candidates rechecked, queries scanned in full (read after the sync)
+    return KG_OK;
+}
+
+}  // namespace kgb

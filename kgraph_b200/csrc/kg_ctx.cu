@@ -7,6 +7,7 @@
 #include <random>
 #include <limits>
 #include "kg_ctx.h"
+#include "kg_bruteforce.h"
 #include "kg_search.h"
 #include "kg_warp.cuh"
 
@@ -484,10 +485,32 @@ int search_locked(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_
         a.cmeta = ctx->cmeta.as<float4>();
     }
 
+    // every query a brute-force query (no graph, or P >= N): the tensor-core path where it applies
+    bool bf_all = !graph || (!P_per_q && params->P >= N);
+    if (graph && P_per_q) {
+        bf_all = true;
+        for (size_t i = 0; i < Q && bf_all; ++i) bf_all = hP[i] >= N;
+    }
+    const bool use_tc_bf = bf_all && !K_per_q && ctx->bf_mode != KG_BRUTEFORCE_SCAN &&
+                           bruteforce_tc_supported(ctx, params->K) &&
+                           (ctx->bf_mode == KG_BRUTEFORCE_TENSOR || N >= 1024) && N == ctx->n;
+    ctx->last_bf = kg_bruteforce_stats{};
+    ctx->bf_stats_dev = nullptr;
+    if (use_tc_bf) {   // the dataset's BF16 rows: once per dataset, outside the timed region
+        const int pr = bruteforce_prepare(ctx);
+        if (pr != KG_OK) return pr;
+    }
     cudaEventRecord(ctx->ev0, ctx->stream);
-    if ((e = launch_search(a, sh, ctx->num_sms, ctx->stream, nullptr)) != cudaSuccess)
+    if (use_tc_bf) {
+        int br = bruteforce_tc(ctx, a.Q, a.q_ld, (uint32_t)Q, params->K, params->epsilon, a.out_ids, a.out_dists,
+                               a.out_count, a.out_cost, (uint32_t)out_ld, a.work);
+        if (br != KG_OK) return br;
+    } else if ((e = launch_search(a, sh, ctx->num_sms, ctx->stream, nullptr)) != cudaSuccess) {
         return cuda_fail(ctx, e, "search launch");
+    }
     cudaEventRecord(ctx->ev1, ctx->stream);
+    unsigned long long bf_h[2] = {0, 0};
+    if (use_tc_bf) cudaMemcpyAsync(bf_h, ctx->bf_stats_dev, 16, cudaMemcpyDeviceToHost, ctx->stream);
 
     if (!ids_dev) cudaMemcpyAsync(ids, a.out_ids, Q * out_ld * 4, cudaMemcpyDeviceToHost, ctx->stream);
     if (dists && !d_dev) cudaMemcpyAsync(dists, a.out_dists, Q * out_ld * 4, cudaMemcpyDeviceToHost, ctx->stream);
@@ -496,12 +519,31 @@ int search_locked(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_
     cudaMemcpyAsync(ctx->last_work, a.work, 32, cudaMemcpyDeviceToHost, ctx->stream);
     if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "search");
     cudaEventElapsedTime(&ctx->last_search_ms, ctx->ev0, ctx->ev1);
+    if (use_tc_bf) {
+        ctx->last_bf.tensor = 1;
+        ctx->last_bf.candidates = bf_h[0];
+        ctx->last_bf.full_scans = bf_h[1];
+    }
     return check_device_error(ctx, "search");
 }
 
 }  // namespace kgb
 
 extern "C" {
+
+int kg_set_bruteforce_mode(kg_ctx *ctx, int mode) {
+    if (!ctx || mode < KG_BRUTEFORCE_AUTO || mode > KG_BRUTEFORCE_TENSOR) return KG_E_INVALID;
+    Lock lk(ctx);
+    ctx->bf_mode = mode;
+    return KG_OK;
+}
+
+int kg_last_bruteforce_stats(kg_ctx *ctx, kg_bruteforce_stats *out) {
+    if (!ctx || !out) return KG_E_INVALID;
+    Lock lk(ctx);
+    *out = ctx->last_bf;
+    return KG_OK;
+}
 
 int kg_search_batch(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes,
                     const kg_search_params *params, const uint32_t *K_per_q, const uint32_t *P_per_q,

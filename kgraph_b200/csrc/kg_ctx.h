@@ -89,6 +89,13 @@ struct kg_ctx {
     kgb::DevBuf tcstat;              // tensor-core join counters
     kgb::DevBuf joinq, joinaux, joinb;   // tensor-core join: candidate queue, worst-case prefix, round bounds
     kg_join_stats last_join{};
+    // tensor-core brute force (kg_bruteforce.cu): BF16 centred rows, row terms, mean + extents, work space
+    kgb::DevBuf bf_rows, bf_meta, bf_aux, bf_work;
+    uint64_t bf_data_version = ~0ull;
+    float bf_ext[5] = {0, 0, 0, 0, 0};
+    int bf_mode = KG_BRUTEFORCE_AUTO;
+    unsigned long long *bf_stats_dev = nullptr;
+    kg_bruteforce_stats last_bf{};
     kgb::RouterState *router = nullptr;   // learned entry router (kg_router.cu)
     void *noalloc_scratch = nullptr;      // device address of kg_search_batch_noalloc's static array
     kgb::DevBuf rseeds;                   // router seeds handed to the search (kg_router_search)

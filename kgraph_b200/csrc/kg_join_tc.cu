@@ -477,8 +477,8 @@ __global__ void __launch_bounds__(256) join_insert_kernel(BuildState s, JoinQueu
         }
     }
     if (lane == 0 && tally.attempts) {
-        atomicAdd(s.inserts, tally.attempts);
-        atomicAdd(s.inserts + 1, tally.landed);
+        atomicAdd(s.inserts, (unsigned long long)tally.attempts);
+        atomicAdd(s.inserts + 1, (unsigned long long)tally.landed);
     }
 }
 
