@@ -41,8 +41,9 @@ UNIT = "queries/s"
 N_BASE, DIM, N_CENTRES, N_QUERIES = 1_000_000, 128, 256, 10_000
 BUILD = dict(K=50, L=100, S=12, R=100, iterations=30, reverse=-1)
 P_LADDER = [100, 200, 300, 500, 700, 1000, 1500, 2000, 3000]
-ROUTER_P_LADDER = [10, 20, 30, 50, 100, 200, 300, 500, 1000]
+ROUTER_P_LADDER = [1, 2, 3, 5, 7, 10, 15, 20, 30, 50, 100, 200, 300, 500, 1000]
 ROUTER_SEEDS = 3          # starting points per query (the reference requires init < K)
+ROUTER_SEED_CHOICES = [1, 2, 3, 5, 9]   # the operating point search tries each (init < K = 10)
 ROUTER_TRAIN = 200_000    # (query, best node) training pairs
 TARGET = 0.95
 # DRAM read + write of one search launch (10,000 queries, K=10) from ncu
@@ -688,29 +689,49 @@ def main():
         t0 = time.perf_counter()
         rinfo = ctx.router_train(Qtrain, clusters=1024, hidden=256, label_P=P_star, epochs=4, batch=1024)
         router_train_s = time.perf_counter() - t0
-        seeds = ctx.router_seeds(Q, ROUTER_SEEDS, out_ld=10)
-        r_ladder = {}
-        P_r = None
-        for P in ROUTER_P_LADDER:
-            ids, _, _, _ = ctx.search(Q, K=10, P=P, init=ROUTER_SEEDS, init_ids=seeds)
-            r_ladder[P] = recall_at(ids, Xt2, Qt, gt_d, 10, torch)
-            if r_ladder[P] >= TARGET:
-                P_r = P
-                break
-        # all ranks agree on the router's P (or that the target was missed), so they take the same
-        # collective steps below
-        NOT_REACHED = ROUTER_P_LADDER[-1] + 1
-        agreed = int(max_over_ranks(NOT_REACHED if P_r is None else P_r, dist, world, "cuda"))
-        P_r = None if agreed == NOT_REACHED else agreed
+        # operating point: for each number of router seeds m, the smallest P of the ladder whose
+        # recall@10 reaches the target; the pair with the fastest step (router seeds + walk, device
+        # time) is the one timed below
+        points = {}
+        for m in ROUTER_SEED_CHOICES:
+            seeds = ctx.router_seeds(Q, m, out_ld=10)
+            ladder_m = {}
+            for P in ROUTER_P_LADDER:
+                ids, _, _, _ = ctx.search(Q, K=10, P=P, init=m, init_ids=seeds)
+                ladder_m[P] = recall_at(ids, Xt2, Qt, gt_d, 10, torch)
+                if ladder_m[P] >= TARGET:
+                    ms = []
+                    for _ in range(3):
+                        s_ms = ctx.router_seeds_raw(capi._ptr(q_dev), N_QUERIES, q_dev.stride(0) * 4, m,
+                                                    capi._ptr(out_i), 10)
+                        ctx.search(Q, K=10, P=P, init=m, init_ids=seeds)
+                        ms.append(s_ms + ctx.timing()[1])
+                    points[m] = {"P": P, "recall@10": ladder_m[P], "ms": min(ms), "ladder": ladder_m}
+                    break
+            else:
+                points[m] = {"P": None, "ladder": ladder_m}
+        reached = [m for m in points if points[m]["P"] is not None]
+        # all ranks agree on (m, P) (or that the target was missed), so they take the same collective
+        # steps below: the encoded choice with the largest code wins
+        NOT_REACHED = 0
+        code = 0
+        if reached:
+            m_best = min(reached, key=lambda m: points[m]["ms"])
+            code = m_best * 100000 + points[m_best]["P"]
+        code = int(max_over_ranks(code, dist, world, "cuda"))
+        P_r = None if code == NOT_REACHED else code % 100000
+        m_r = code // 100000 if code else ROUTER_SEEDS
+        seeds = ctx.router_seeds(Q, m_r, out_ld=10)
+        r_ladder = dict(points.get(m_r, {}).get("ladder", {}))
         if P_r is not None and P_r not in r_ladder:
-            ids, _, _, _ = ctx.search(Q, K=10, P=P_r, init=ROUTER_SEEDS, init_ids=seeds)
+            ids, _, _, _ = ctx.search(Q, K=10, P=P_r, init=m_r, init_ids=seeds)
             r_ladder[P_r] = recall_at(ids, Xt2, Qt, gt_d, 10, torch)
         if P_r is not None:
-            rparams = capi.SearchParams(10, 0, P_r, 10, 1, 1e30, 1998, ROUTER_SEEDS)
-            tune_router = ctx.search_autotune(Q, K=10, P=P_r, init=ROUTER_SEEDS, init_ids=seeds)
+            rparams = capi.SearchParams(10, 0, P_r, 10, 1, 1e30, 1998, m_r)
+            tune_router = ctx.search_autotune(Q, K=10, P=P_r, init=m_r, init_ids=seeds)
 
             def step_router():
-                ms_r = ctx.router_seeds_raw(capi._ptr(q_dev), N_QUERIES, q_dev.stride(0) * 4, ROUTER_SEEDS,
+                ms_r = ctx.router_seeds_raw(capi._ptr(q_dev), N_QUERIES, q_dev.stride(0) * 4, m_r,
                                             capi._ptr(out_i), 10)
                 ctx.search_raw(capi._ptr(q_dev), N_QUERIES, q_dev.stride(0) * 4, rparams, None, None, 10,
                                capi._ptr(out_i), capi._ptr(out_d), capi._ptr(out_c), None)
@@ -741,7 +762,9 @@ def main():
                 if it >= args.warmup:
                     r_e2e_ms.append(1000 * (time.perf_counter() - t0))
             r_e2e, _ = replica_throughput(sum(r_e2e_ms), N_QUERIES, args.steps, dist, world, "cuda")
-            router = {"value": r_value, "unit": UNIT, "P": P_r, "seeds_per_query": ROUTER_SEEDS,
+            router = {"value": r_value, "unit": UNIT, "P": P_r, "seeds_per_query": m_r,
+                      "operating_points": {str(m): {k: v for k, v in pt.items() if k != "ladder"}
+                                           for m, pt in points.items()},
                       "recall@10": r_ladder[P_r], "recall_ladder": r_ladder, "ms_per_step": sum(r_ms) / args.steps,
                       "e2e": r_e2e, "train_s": router_train_s, "train": rinfo,
                       "speedup_vs_plain": r_value / value, "search_ms_per_step": sum(r_search_ms) / args.steps,
@@ -813,7 +836,8 @@ def main():
                 "plain": plain, "router": router,
                 "config": {"workload": "1M x 128 mixture (256 centres), 10k queries, K=10, P=%d%s" % (
                                router["P"] if best_router else P_star,
-                               ", %d learned init seeds per query" % ROUTER_SEEDS if best_router else ""),
+                               ", %d learned init seeds per query" % router["seeds_per_query"] if best_router
+                               else ""),
                            "N": args.n, "D": DIM, "queries": N_QUERIES, "K": 10,
                            "P": router["P"] if best_router else P_star, "build": BUILD,
                            "l2": "flushed between steps; dataset 512 MB > L2",
