@@ -2,7 +2,7 @@
 
     libkgraph_b200.so   CUDA kernels + C-ABI (include/kgraph_b200.h) + C++ API (include/kgraph.h)
     _kgraph*.so         Python module (pybind11) over the C++ API
-    bin/index, bin/search   the command-line tools (the reference's index / search), over the C++ API
+    bin/index, bin/search, bin/prune, bin/resave   the command-line tools (the reference's), over the C++ API
 
 Run as ``python -m kgraph_b200.build`` or through ``__graft_entry__.build()``.
 nvcc cross-compiles without a GPU.
@@ -77,7 +77,7 @@ def build(verbose=False):
     bindir = os.path.join(PKG, "bin")
     os.makedirs(bindir, exist_ok=True)
     cli = os.path.join(PKG, "cli")
-    for tool in ("index", "search"):
+    for tool in ("index", "search", "prune", "resave"):
         src = os.path.join(cli, tool + ".cpp")
         exe = os.path.join(bindir, tool)
         if _stale(exe, [src, LIB, os.path.join(cli, "cli_args.h")] + HEADERS):

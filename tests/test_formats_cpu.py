@@ -54,3 +54,7 @@ def test_cli_tools_usage_and_options():
     assert r.returncode == 0 and r.stdout.startswith("search <data> <index> <query> [output]")
     r = subprocess.run([os.path.join(binp, "index"), "--bogus", "1", "x"], capture_output=True, text=True)
     assert r.returncode != 0 and "unrecognised option" in r.stderr
+    r = subprocess.run([os.path.join(binp, "prune"), "-h"], capture_output=True, text=True)
+    assert r.returncode == 0 and r.stdout.startswith("Usage: prune [OTHER OPTIONS]... DATA INPUT [OUTPUT]")
+    r = subprocess.run([os.path.join(binp, "resave")], capture_output=True, text=True)
+    assert r.returncode == 0 and "--no-dist" in r.stdout

@@ -92,3 +92,40 @@ def test_cli_index_and_search_match_reference_search(tmp_path):
     ref_ids, _, _, ref_cost = ref.search_l2sqr(X, str(tmp_path / "g.idx"), Q, K=10, P=30)
     assert (res == ref_ids).all()                                     # the reference's walk on the tool's index
     assert abs(float(m.group(3)) - float(ref_cost.mean())) < 1e-5
+
+
+@pytest.mark.parametrize("level", [1, 2])
+def test_cli_resave_and_prune_tools(tmp_path, level):
+    """The reference's resave and prune tools (resave.cpp, prune.cpp): resave
+    --no-dist writes the reference's no-dist bytes; --prune and the prune tool
+    prune exactly as the reference's prune (the pinned oracle restatement);
+    the prune tool's default level is the reference's PRUNE_LEVEL_1 &
+    PRUNE_LEVEL_2 = 0, a plain re-save."""
+    binp = os.path.join(ROOT, "kgraph_b200", "bin")
+    g = load_golden("u16")
+    f = np.load(os.path.join(GOLDEN, "formats_u16.npz"))
+    src = tmp_path / "in.idx"
+    src.write_bytes(g["index_bytes"].tobytes())
+    r = subprocess.run([os.path.join(binp, "resave"), str(src), str(tmp_path / "nd.idx"), "--no-dist"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert (tmp_path / "nd.idx").read_bytes() == f["nodist_bytes"].tobytes()
+    G = ko.read_index(g["index_bytes"])
+    R = ko.Oracle(g["X"], g["metric"]).prune(G, level)
+    r = subprocess.run([os.path.join(binp, "resave"), str(src), str(tmp_path / "pr.idx"), "--prune", str(level)],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    P = ko.read_index(str(tmp_path / "pr.idx"))
+    assert (P.offsets == R.offsets).all() and (P.ids == R.ids).all() and (P.M == R.M).all()
+    assert (P.dists.view(np.uint32) == R.dists.view(np.uint32)).all()
+    _lshkit(tmp_path / "data", g["X"].astype(np.float32))
+    r = subprocess.run([os.path.join(binp, "prune"), str(tmp_path / "data"), str(src), str(tmp_path / "p2.idx"),
+                        "--prune", str(level)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    P2 = ko.read_index(str(tmp_path / "p2.idx"))
+    assert (P2.offsets == R.offsets).all() and (P2.ids == R.ids).all() and (P2.M == R.M).all()
+    r = subprocess.run([os.path.join(binp, "prune"), str(tmp_path / "data"), str(src), str(tmp_path / "p0.idx")],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    P0 = ko.read_index(str(tmp_path / "p0.idx"))
+    assert (P0.offsets == G.offsets).all() and (P0.ids == G.ids).all() and (P0.M == G.M).all()
