@@ -467,7 +467,7 @@ __global__ void __launch_bounds__(256) bf_recheck_kernel(DataView D, const float
 
 bool bruteforce_tc_supported(const kg_ctx *ctx, uint32_t K) {
     if (K == 0 || K > BF_MAX_K || ctx->ld > 256) return false;
-    return bruteforce_tc_smem(ctx->ld, K) <= 200 * 1024;
+    return bruteforce_tc_smem(ctx->ld, K) <= 224 * 1024;   // the sweep's dynamic shared memory (227 KB max)
 }
 
 // Dynamic shared memory of a sweep CTA: the query tile, two row tiles, the

@@ -229,10 +229,13 @@ __global__ void __launch_bounds__(256) join_kernel(BuildState s) {
         auto settle = [&](bool valid, uint32_t x, uint32_t y, float dd) {
             const float rx = (valid && t == 0) ? *reinterpret_cast<volatile float *>(s.radius + x) : 0.f;
             const float ry = (valid && t == 1) ? *reinterpret_cast<volatile float *>(s.radius + y) : 0.f;
-            unsigned vm = __ballot_sync(FULL, valid && t == 0);
+            const unsigned vm_all = __ballot_sync(FULL, valid && t == 0);
             const unsigned nx = __ballot_sync(FULL, valid && t == 0 && !(dd > rx));
             const unsigned ny = __ballot_sync(FULL, valid && t == 1 && !(dd > ry));
-            comps += __popc(vm);
+            comps += __popc(vm_all);
+            // only the pairs with an offer that passed a radius test: a pair both endpoints reject
+            // inserts nothing and leaves r at pool.size() (>= K)
+            unsigned vm = nx | (ny >> 1);
             while (vm) {
                 const int src = __ffs(vm) - 1;
                 vm &= vm - 1;
@@ -275,8 +278,8 @@ __global__ void __launch_bounds__(256) join_kernel(BuildState s) {
     }
     if (lane == 0 && comps) atomicAdd(s.n_comps, comps);
     if (lane == 0 && tally.attempts) {
-        atomicAdd(s.inserts, (unsigned long long)tally.attempts);
-        atomicAdd(s.inserts + 1, (unsigned long long)tally.landed);
+        atomicAdd(s.inserts, tally.attempts);
+        atomicAdd(s.inserts + 1, tally.landed);
     }
 }
 

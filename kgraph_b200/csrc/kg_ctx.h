@@ -85,6 +85,7 @@ struct kg_ctx {
     std::vector<uint32_t> h_stage_u32;
 
     kgb::DevBuf build_scratch[25];   // NN-descent state (kg_build.cu)
+    kgb::DevBuf rev_scratch[17];     // reverse-edge completion work space (kg_graph.cu), kept between builds
     int join_mode = KG_JOIN_AUTO;
     kgb::DevBuf tcstat;              // tensor-core join counters
     kgb::DevBuf joinq, joinaux, joinb;   // tensor-core join: candidate queue, worst-case prefix, round bounds

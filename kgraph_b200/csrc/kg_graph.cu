@@ -172,17 +172,19 @@ int graph_reverse(kg_ctx *ctx, int rev_k) {
     const size_t n = N;
     cudaStream_t st = ctx->stream;
     cudaError_t e;
-    DevBuf kcnt, koff, rc, toff, deg, noff, fdeg, foff, key, val, skey, sval, tmp, ai, ad, fi, fd;
-    auto fail = [&](const char *w) {
-        DevBuf *all[] = {&kcnt, &koff, &rc, &toff, &deg, &noff, &fdeg, &foff, &key, &val, &skey, &sval, &tmp,
-                         &ai, &ad, &fi, &fd};
-        for (DevBuf *b : all) b->release();
-        return cuda_fail(ctx, e, w);
-    };
-    if ((e = kcnt.reserve((n + 1) * 8)) != cudaSuccess || (e = koff.reserve((n + 1) * 8)) != cudaSuccess ||
-        (e = rc.reserve((n + 1) * 8)) != cudaSuccess || (e = toff.reserve((n + 1) * 8)) != cudaSuccess ||
-        (e = deg.reserve((n + 1) * 8)) != cudaSuccess || (e = noff.reserve((n + 1) * 8)) != cudaSuccess ||
-        (e = fdeg.reserve((n + 1) * 8)) != cudaSuccess || (e = foff.reserve((n + 1) * 8)) != cudaSuccess)
+    // Work space kept in the context between calls: a build reverses once per call, and freeing and
+    // re-allocating ~2 GB (1M nodes) each time costs device-synchronising cudaFree / cudaMalloc calls whose
+    // time varied from build to build.  Buffers grow with 1/8 slack.
+    DevBuf *R = ctx->rev_scratch;
+    DevBuf &kcnt = R[0], &koff = R[1], &rc = R[2], &toff = R[3], &deg = R[4], &noff = R[5], &fdeg = R[6],
+           &foff = R[7], &key = R[8], &val = R[9], &skey = R[10], &sval = R[11], &tmp = R[12], &ai = R[13],
+           &ad = R[14], &fi = R[15], &fd = R[16];
+    auto grow = [](DevBuf &b, size_t bytes) { return b.reserve(bytes <= b.bytes ? bytes : bytes + bytes / 8); };
+    auto fail = [&](const char *w) { return cuda_fail(ctx, e, w); };
+    if ((e = grow(kcnt, (n + 1) * 8)) != cudaSuccess || (e = grow(koff, (n + 1) * 8)) != cudaSuccess ||
+        (e = grow(rc, (n + 1) * 8)) != cudaSuccess || (e = grow(toff, (n + 1) * 8)) != cudaSuccess ||
+        (e = grow(deg, (n + 1) * 8)) != cudaSuccess || (e = grow(noff, (n + 1) * 8)) != cudaSuccess ||
+        (e = grow(fdeg, (n + 1) * 8)) != cudaSuccess || (e = grow(foff, (n + 1) * 8)) != cudaSuccess)
         return fail("alloc reverse");
     cudaMemsetAsync(kcnt.p, 0, (n + 1) * 8, st);
     cudaMemsetAsync(rc.p, 0, (n + 1) * 8, st);
@@ -196,8 +198,8 @@ int graph_reverse(kg_ctx *ctx, int rev_k) {
     cudaMemcpyAsync(&Ef, koff.as<uint64_t>() + N, 8, cudaMemcpyDeviceToHost, st);
     cudaStreamSynchronize(st);
     if (Ef >= 0xFFFFFFFFull) { e = cudaErrorInvalidValue; return fail("graph too large to reverse"); }
-    if ((e = key.reserve(Ef * 4 + 4)) != cudaSuccess || (e = val.reserve(Ef * 4 + 4)) != cudaSuccess ||
-        (e = skey.reserve(Ef * 4 + 4)) != cudaSuccess || (e = sval.reserve(Ef * 4 + 4)) != cudaSuccess)
+    if ((e = grow(key, Ef * 4 + 4)) != cudaSuccess || (e = grow(val, Ef * 4 + 4)) != cudaSuccess ||
+        (e = grow(skey, Ef * 4 + 4)) != cudaSuccess || (e = grow(sval, Ef * 4 + 4)) != cudaSuccess)
         return fail("alloc reverse");
     rev_edges_kernel<<<grid * 2, 256, 0, st>>>(N, ctx->offsets.as<uint64_t>(), ctx->nbr.as<uint32_t>(),
                                                koff.as<uint64_t>(), key.as<uint32_t>(), val.as<uint32_t>(),
@@ -208,7 +210,7 @@ int graph_reverse(kg_ctx *ctx, int rev_k) {
     size_t tb = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, tb, key.as<uint32_t>(), skey.as<uint32_t>(), val.as<uint32_t>(),
                                     sval.as<uint32_t>(), (int64_t)Ef, 0, end_bit, st);
-    if ((e = tmp.reserve(tb)) != cudaSuccess) return fail("alloc sort");
+    if ((e = grow(tmp, tb)) != cudaSuccess) return fail("alloc sort");
     if ((e = cub::DeviceRadixSort::SortPairs(tmp.p, tb, key.as<uint32_t>(), skey.as<uint32_t>(), val.as<uint32_t>(),
                                              sval.as<uint32_t>(), (int64_t)Ef, 0, end_bit, st)) != cudaSuccess)
         return fail("sort");
@@ -216,7 +218,7 @@ int graph_reverse(kg_ctx *ctx, int rev_k) {
     rev_degree_kernel<<<grid, 256, 0, st>>>(N, kcnt.as<uint64_t>(), rc.as<uint64_t>(), deg.as<uint64_t>());
     if ((e = scan_counts64(ctx, deg.as<uint64_t>(), noff.as<uint64_t>(), N)) != cudaSuccess) return fail("scan");
     const uint64_t E2 = 2 * Ef;
-    if ((e = ai.reserve(E2 * 4 + 4)) != cudaSuccess || (e = ad.reserve(E2 * 4 + 4)) != cudaSuccess)
+    if ((e = grow(ai, E2 * 4 + 4)) != cudaSuccess || (e = grow(ad, E2 * 4 + 4)) != cudaSuccess)
         return fail("alloc reverse");
     std::cerr << "Reranking edges..." << std::endl;
     rev_assemble_kernel<<<(N + 127) / 128, 128, 0, st>>>(
@@ -228,7 +230,7 @@ int graph_reverse(kg_ctx *ctx, int rev_k) {
     uint64_t Efin = 0;
     cudaMemcpyAsync(&Efin, foff.as<uint64_t>() + N, 8, cudaMemcpyDeviceToHost, st);
     cudaStreamSynchronize(st);
-    if ((e = fi.reserve(Efin * 4 + 4)) != cudaSuccess || (e = fd.reserve(Efin * 4 + 4)) != cudaSuccess)
+    if ((e = grow(fi, Efin * 4 + 4)) != cudaSuccess || (e = grow(fd, Efin * 4 + 4)) != cudaSuccess)
         return fail("alloc reverse");
     compact_kernel<<<grid * 2, 256, 0, st>>>(N, noff.as<uint64_t>(), foff.as<uint64_t>(), ai.as<uint32_t>(),
                                              ad.as<float>(), fi.as<uint32_t>(), fd.as<float>(),
@@ -238,9 +240,6 @@ int graph_reverse(kg_ctx *ctx, int rev_k) {
     swap_graph(ctx, foff, fi, fd);
     ctx->E = Efin;
     ++ctx->graph_version;
-    DevBuf *all[] = {&kcnt, &koff, &rc, &toff, &deg, &noff, &fdeg, &foff, &key, &val, &skey, &sval, &tmp,
-                     &ai, &ad, &fi, &fd};
-    for (DevBuf *b : all) b->release();
     return check_device_error(ctx, "reverse");
 }
 

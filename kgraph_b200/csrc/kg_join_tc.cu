@@ -461,9 +461,9 @@ __global__ void __launch_bounds__(256) join_insert_kernel(BuildState s, JoinQueu
         const float dd = pair_dist(s.D, x, y, t, FULL);
         const float rx = (valid && t == 0) ? *reinterpret_cast<volatile float *>(s.radius + x) : 0.f;
         const float ry = (valid && t == 1) ? *reinterpret_cast<volatile float *>(s.radius + y) : 0.f;
-        unsigned vm = __ballot_sync(FULL, valid && t == 0);
         const unsigned nx = __ballot_sync(FULL, valid && t == 0 && !(dd > rx));
         const unsigned ny = __ballot_sync(FULL, valid && t == 1 && !(dd > ry));
+        unsigned vm = nx | (ny >> 1);   // pairs with an offer that passed a radius test
         while (vm) {
             const int src = __ffs(vm) - 1;
             vm &= vm - 1;
