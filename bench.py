@@ -303,9 +303,10 @@ WORKLOADS = {
                     "BF16 search filter; 10k queries, K=10", n=1_000_000, d=96, kind="sphere", centres=1000, metric="angular",
                nq=10_000, build=dict(BUILD), P_ladder=P_LADDER, join="bf16", search_precision="bf16"),
     "c4": dict(desc="2M x 128 mixture (256 centres); 100k queries in one launch, K from {1,10,100}, "
-                    "P from {50,100,200}; per-batch latency over 1k-query batches; FP8 E4M3 search filter",
+                    "P from {50,100,200}; per-batch latency over 1k-query batches; FP8 E4M3 tensor-core join "
+                    "tiles (per-row scales, FP32 recheck) and FP8 E4M3 search filter",
                n=2_000_000, d=128, kind="mixture", centres=256, metric="euclidean", nq=100_000,
-               build=dict(BUILD), join="auto", mixed=True, search_precision="fp8"),
+               build=dict(BUILD), join="fp8", mixed=True, search_precision="fp8"),
     "c5": dict(desc="5M x 128 mixture (4096 centres), graph K=50; router (200k training pairs) vs plain "
                     "seeded walk on 50k held-out queries, K=10", n=5_000_000, d=128, kind="mixture", centres=4096,
                metric="euclidean", nq=50_000, build=dict(BUILD),

@@ -311,13 +311,18 @@ int kg_tc_assign_check(kg_ctx *ctx, const uint16_t *F, int n, int D, const uint1
  *                 least half of the pools full (before that every pair passes
  *                 the radius test and the FP32 join is the cheaper path);
  *   KG_JOIN_BF16_ALWAYS  the BF16 filter in every iteration;
+ *   KG_JOIN_FP8 / KG_JOIN_FP8_ALWAYS  the same filter with FP8 E4M3 tiles and a
+ *                 scale per row (max |x_u - x_n| / 448); the margin adds each
+ *                 row's exact quantisation error ||v - scale q|| (FP64) relative
+ *                 to ||v||; needs d padded to a multiple of 32;
  *   KG_JOIN_AUTO  (default) the faster path measured for the build's own
  *                 workloads: KG_JOIN_FP32 (the join is bound by the locked
  *                 pool inserts, which the filter does not reduce). */
-enum { KG_JOIN_AUTO = 0, KG_JOIN_FP32 = 1, KG_JOIN_BF16 = 2, KG_JOIN_BF16_ALWAYS = 3 };
+enum { KG_JOIN_AUTO = 0, KG_JOIN_FP32 = 1, KG_JOIN_BF16 = 2, KG_JOIN_BF16_ALWAYS = 3, KG_JOIN_FP8 = 4,
+       KG_JOIN_FP8_ALWAYS = 5 };
 int kg_set_join_precision(kg_ctx *ctx, int mode);
-/* Counters of the last kg_build's join.  mode: KG_JOIN_BF16 when any
- * iteration ran the tensor-core filter (tc_iterations of them).  pairs: join
+/* Counters of the last kg_build's join.  mode: KG_JOIN_BF16 or KG_JOIN_FP8 when
+ * any iteration ran the tensor-core filter (tc_iterations of them).  pairs: join
  * pairs (IndexInfo.cost * N(N-1)/2 summed over iterations); rechecked: pairs
  * recomputed in FP32 after the BF16 filter.  On a sample of nodes every pair
  * is also evaluated in FP64: sampled pairs, the BF16 tile distance's absolute

@@ -27,7 +27,7 @@ SYMBOLS = [
     "kg_last_build_iterations", "kg_set_bruteforce_mode", "kg_last_bruteforce_stats",
 ]
 
-JOIN = {"auto": 0, "fp32": 1, "bf16": 2, "bf16_always": 3}
+JOIN = {"auto": 0, "fp32": 1, "bf16": 2, "bf16_always": 3, "fp8": 4, "fp8_always": 5}
 
 
 class IndexParams(C.Structure):
@@ -385,7 +385,7 @@ class Context:
         st = JoinStats()
         self._check(self.L.kg_last_join_stats(self.h, C.byref(st)))
         out = {f: getattr(st, f) for f, _ in JoinStats._fields_}
-        out["mode"] = {1: "fp32", 2: "bf16"}.get(st.mode, "none")
+        out["mode"] = {1: "fp32", 2: "bf16", 4: "fp8"}.get(st.mode, "none")
         return out
 
     def search_autotune(self, Q, K=10, P=100, M=0, S=10, T=1, epsilon=1e30, seed=1998, K_per_q=None, P_per_q=None,

@@ -670,9 +670,13 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
     if ((e = ctx->tcstat.reserve(sizeof(JoinTcStats))) != cudaSuccess) return cuda_fail(ctx, e, "alloc build state");
     s.tc = ctx->tcstat.as<JoinTcStats>();
     cudaMemsetAsync(s.tc, 0, sizeof(JoinTcStats), st);
-    const bool use_tc = ctx->join_mode == KG_JOIN_BF16 || ctx->join_mode == KG_JOIN_BF16_ALWAYS;
-    if (use_tc && !join_tc_supported(s))
-        return set_error(ctx, KG_E_INVALID, "tensor-core join: lists do not fit in shared memory");
+    const bool fp8 = ctx->join_mode == KG_JOIN_FP8 || ctx->join_mode == KG_JOIN_FP8_ALWAYS;
+    const bool use_tc = fp8 || ctx->join_mode == KG_JOIN_BF16 || ctx->join_mode == KG_JOIN_BF16_ALWAYS;
+    const bool tc_always = ctx->join_mode == KG_JOIN_BF16_ALWAYS || ctx->join_mode == KG_JOIN_FP8_ALWAYS;
+    if (use_tc && !join_tc_supported(s, fp8 ? 1 : 0))
+        return set_error(ctx, KG_E_INVALID, fp8 ? "tensor-core join (FP8): needs d padded to a multiple of 32 and "
+                                                  "lists that fit in shared memory"
+                                                : "tensor-core join: lists do not fit in shared memory");
     JoinQueue jq{};
     uint64_t *jworst = nullptr, *jpre = nullptr, qcap = 0;
     if (use_tc) {
@@ -808,7 +812,7 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
         // The tensor-core filter can only skip pairs against finite radii: while
         // most pools are still filling, every pair passes it and the fused
         // CUDA-core join is the cheaper path.
-        const bool tc_now = use_tc && (ctx->join_mode == KG_JOIN_BF16_ALWAYS || full_frac >= JOIN_TC_MIN_FULL);
+        const bool tc_now = use_tc && (tc_always || full_frac >= JOIN_TC_MIN_FULL);
         if (tc_now) {
             ++tc_iters;
             if (pending_update && (e = run_graph(g_update, rec_update)) != cudaSuccess)
@@ -826,7 +830,7 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
             jq.bounds = ctx->joinb.as<uint32_t>();
             if ((e = join_tc_bounds(st, jpre, N, slab, R, jq.bounds)) != cudaSuccess) return cuda_fail(ctx, e, "join");
             for (uint32_t r = 0; r < R; ++r)
-                if ((e = launch_join_tc(ctx->num_sms, grid_for(ctx), st, s, jq, r)) != cudaSuccess)
+                if ((e = launch_join_tc(ctx->num_sms, grid_for(ctx), st, s, jq, r, fp8 ? 1 : 0)) != cudaSuccess)
                     return cuda_fail(ctx, e, "join");
             if ((e = run_graph(g_stats, rec_stats)) != cudaSuccess) return cuda_fail(ctx, e, "statistics graph");
         } else if (pending_update) {
@@ -937,7 +941,7 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
     cudaEventElapsedTime(&ctx->last_build_ms, ctx->ev0, ctx->ev1);
     kg_join_stats &js = ctx->last_join;
     js = kg_join_stats{};
-    js.mode = tc_iters ? KG_JOIN_BF16 : KG_JOIN_FP32;
+    js.mode = tc_iters ? (fp8 ? KG_JOIN_FP8 : KG_JOIN_BF16) : KG_JOIN_FP32;
     js.tc_iterations = tc_iters;
     js.pairs = hstat_prev;
     js.rechecked = ts.rechecked + fp32_pairs;
@@ -975,7 +979,7 @@ extern "C" int kg_last_build_work(kg_ctx *ctx, uint64_t *pairs, uint64_t *list_e
 }
 
 extern "C" int kg_set_join_precision(kg_ctx *ctx, int mode) {
-    if (!ctx || mode < KG_JOIN_AUTO || mode > KG_JOIN_BF16_ALWAYS) return KG_E_INVALID;
+    if (!ctx || mode < KG_JOIN_AUTO || mode > KG_JOIN_FP8_ALWAYS) return KG_E_INVALID;
     std::lock_guard<std::mutex> guard(ctx->mu);
     ctx->join_mode = mode;
     return KG_OK;

@@ -61,16 +61,17 @@ constexpr int JOIN_TC_MAX_CTAS_PER_SM = 3;
 constexpr double JOIN_TC_MIN_FULL = 0.5;
 
 // One round of the tensor-core local join (kg_join_tc.cu): the filter over the
-// round's nodes, then the inserts of the queued pairs.
+// round's nodes (prec 0: BF16 tiles; 1: E4M3 tiles with per-row scales), then
+// the inserts of the queued pairs.
 cudaError_t launch_join_tc(int num_sms, int grid_insert, cudaStream_t st, const BuildState &s, JoinQueue jq,
-                           uint32_t round);
+                           uint32_t round, int prec);
 // worst[n] = node n's largest pair count (n < N), worst[N] = 0.
 cudaError_t join_tc_worst(cudaStream_t st, const BuildState &s, uint64_t *worst);
 // bounds[0..R] from the exclusive prefix `pre` of worst (R rounds of <= slab).
 cudaError_t join_tc_bounds(cudaStream_t st, const uint64_t *pre, uint32_t N, uint64_t slab, uint32_t R,
                            uint32_t *bounds);
 // Whether the tensor-core join supports this state (shared memory fits).
-bool join_tc_supported(const BuildState &s);
+bool join_tc_supported(const BuildState &s, int prec);
 // Largest number of join pairs one node can produce.
 uint64_t join_tc_node_max(const BuildState &s);
 

@@ -38,6 +38,8 @@
 #include <algorithm>
 #include <cfloat>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_fp8.h>
 #include "kg_build.h"
 #include "kg_insert.cuh"
 #include "kg_tc.cuh"
@@ -103,18 +105,100 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
 }
 
 struct TcShared {
-    uint8_t *bbuf, *abuf;   // two 128-row BF16 tiles, K-major core-matrix layout
+    uint8_t *bbuf, *abuf;   // two 128-row tiles (BF16 or E4M3), K-major core-matrix layout
     float *xn;              // x_n, FP32
     uint32_t *uid;          // U ids (NO_ID for a bad id)
     float *ht, *cc, *nu, *rad;   // per U row: h, c, canonical norm term, radius snapshot
+    float *scl, *rel;       // E4M3 tiles: per U row the scale and ||v - scale q|| / ||v||
 };
 
 // Rows [u0, u0 + rows) of U into `buf` (all 128 tile rows written; rows past
 // `rows` are zero).  Warp w stages row groups w, w+8: lane l owns row
 // (l & 7) of the group and 16-byte chunks (l >> 3) + 4i, so each quarter-warp
 // store covers one contiguous 128-byte core matrix.
+template <int PREC>
 __device__ void stage_rows(const BuildState &s, const TcShared &sh, uint8_t *buf, uint32_t u0, uint32_t rows,
-                           int warp, int lane) {
+                           int warp, int lane);
+
+// E4M3 rows with a per-row scale: v = x_u - x_n in FP32 (as the BF16 rows),
+// scale = max|v| / 448, q = e4m3_satfinite(v / scale); per row the exact
+// ||v - scale q|| (FP64, every term exact there) relative to ||v||, rounded up.
+// Lane l owns row (l & 7) of a group of 8 and 16-byte chunks (16 elements)
+// (l >> 3) + 4i; the row's maximum needs a first pass over its elements.
+template <>
+__device__ void stage_rows<1>(const BuildState &s, const TcShared &sh, uint8_t *buf, uint32_t u0, uint32_t rows,
+                              int warp, int lane) {
+    const uint32_t Dp = s.D.ld, nk16 = Dp >> 4;
+    for (uint32_t g = warp; g * 8 < rows; g += TC_THREADS / 32) {
+        const uint32_t rl = g * 8 + (lane & 7);
+        const bool valid = rl < rows;
+        const uint32_t id = valid ? sh.uid[u0 + rl] : NO_ID;
+        const bool ok = id != NO_ID;
+        float nrm = 0.f, rd = -FLT_MAX;
+        if (ok && lane < 8) {
+            nrm = s.D.norms[id];
+            rd = *reinterpret_cast<volatile const float *>(s.radius + id);
+        }
+        const float *row = s.D.X + (size_t)(ok ? id : 0u) * Dp;
+        float hs = 0.f, cs = 0.f, mx = 0.f;
+        for (uint32_t k16 = lane >> 3; k16 < nk16; k16 += 4) {
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                const float4 n0 = *reinterpret_cast<const float4 *>(sh.xn + 16 * k16 + 4 * h);
+                const float4 a0 = ok ? ld4(row + 16 * k16 + 4 * h) : n0;
+                const float e0 = a0.x - n0.x, e1 = a0.y - n0.y, e2 = a0.z - n0.z, e3 = a0.w - n0.w;
+                hs += e0 * e0 + e1 * e1 + e2 * e2 + e3 * e3;
+                cs += e0 * n0.x + e1 * n0.y + e2 * n0.z + e3 * n0.w;
+                mx = fmaxf(mx, fmaxf(fmaxf(fabsf(e0), fabsf(e1)), fmaxf(fabsf(e2), fabsf(e3))));
+            }
+        }
+        hs += __shfl_xor_sync(FULL, hs, 8);
+        hs += __shfl_xor_sync(FULL, hs, 16);
+        cs += __shfl_xor_sync(FULL, cs, 8);
+        cs += __shfl_xor_sync(FULL, cs, 16);
+        mx = fmaxf(mx, __shfl_xor_sync(FULL, mx, 8));
+        mx = fmaxf(mx, __shfl_xor_sync(FULL, mx, 16));
+        const float scale = mx > 0.f ? mx / 448.f : 1.f;
+        double err2 = 0.0;
+        for (uint32_t k16 = lane >> 3; k16 < nk16; k16 += 4) {
+            uint32_t wv[4];
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                const float4 n0 = *reinterpret_cast<const float4 *>(sh.xn + 16 * k16 + 4 * h);
+                const float4 a0 = ok ? ld4(row + 16 * k16 + 4 * h) : n0;
+                const float e[4] = {a0.x - n0.x, a0.y - n0.y, a0.z - n0.z, a0.w - n0.w};
+                uint32_t word = 0;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const __nv_fp8_storage_t qv = __nv_cvt_float_to_fp8(e[i] / scale, __NV_SATFINITE, __NV_E4M3);
+                    const double y = (double)__half2float(__half(__nv_cvt_fp8_to_halfraw(qv, __NV_E4M3))) * (double)scale;
+                    const double df = (double)e[i] - y;
+                    err2 += df * df;
+                    word |= (uint32_t)qv << (8 * i);
+                }
+                wv[h] = word;
+            }
+            *reinterpret_cast<uint4 *>(buf + tc::kmajor_off8(rl, 16 * k16, Dp)) = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+        }
+        err2 += __shfl_xor_sync(FULL, err2, 8);
+        err2 += __shfl_xor_sync(FULL, err2, 16);
+        if (lane < 8 && valid) {
+            const uint32_t u = u0 + rl;
+            sh.ht[u] = 0.5f * hs;
+            sh.cc[u] = cs;
+            sh.nu[u] = nrm;
+            sh.rad[u] = rd;
+            sh.scl[u] = scale;
+            // relative to ||v|| (hs carries an FP32 rounding: one more relative step of slack)
+            sh.rel[u] = hs > 0.f ? __double2float_ru(sqrt(err2) / sqrt((double)hs) * (1.0 + 1e-5)) : 0.f;
+        }
+    }
+    tc::fence_async_shared();   // make the generic-proxy stores visible to the MMA
+}
+
+template <>
+__device__ void stage_rows<0>(const BuildState &s, const TcShared &sh, uint8_t *buf, uint32_t u0, uint32_t rows,
+                              int warp, int lane) {
     const uint32_t Dp = s.D.ld, nk8 = Dp >> 3;
     // Rows past `rows` are left as they are: the MMA reads them, but their
     // products land only in masked rows / columns of the accumulator.
@@ -167,6 +251,7 @@ __device__ void stage_rows(const BuildState &s, const TcShared &sh, uint8_t *buf
     tc::fence_async_shared();   // make the generic-proxy stores visible to the MMA
 }
 
+template <int PREC>
 __global__ void __launch_bounds__(TC_THREADS, 3) join_tc_kernel(BuildState s, uint32_t Umax, JoinQueue jq,
                                                                   uint32_t round) {
     extern __shared__ __align__(1024) uint8_t smem[];
@@ -179,7 +264,7 @@ __global__ void __launch_bounds__(TC_THREADS, 3) join_tc_kernel(BuildState s, ui
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t Dp = s.D.ld, N = s.D.n;
     const uint32_t n_begin = jq.bounds[round], n_end = jq.bounds[round + 1];
-    const uint32_t tile_bytes = TC_M * Dp * 2;
+    const uint32_t tile_bytes = TC_M * Dp * (PREC ? 1 : 2);
     TcShared sh;
     sh.bbuf = smem;
     sh.abuf = smem + tile_bytes;
@@ -189,6 +274,8 @@ __global__ void __launch_bounds__(TC_THREADS, 3) join_tc_kernel(BuildState s, ui
     sh.cc = sh.ht + Umax;
     sh.nu = sh.cc + Umax;
     sh.rad = sh.nu + Umax;
+    sh.scl = sh.rad + Umax;
+    sh.rel = sh.scl + Umax;
 
     if (warp == 0) tc::tmem_alloc(&tmem_base, TC_TMEM_COLS);
     if (tid == 0) tc::mbar_init(&mbar, 1);
@@ -198,6 +285,8 @@ __global__ void __launch_bounds__(TC_THREADS, 3) join_tc_kernel(BuildState s, ui
     const uint32_t tmem = tmem_base;
     const int q = warp & 3, half = warp >> 2;
     const float et = 0.00390625f + 7.63e-6f + (float)(s.D.d + 4) * 1.1921e-7f;   // 2^-8 + 2^-17 + (D+4) 2^-23
+    // E4M3 tiles: the products' FP32 accumulation, allowed 2^-20 per add, and the two scale multiplies
+    const float g8 = (float)(s.D.d + 4) * 9.5367e-7f + 8.f * 5.9605e-8f;
     const float gam = (float)(s.D.d + 4) * 5.9605e-8f;                             // (D+4) 2^-24
     const int metric = s.D.metric;
     uint32_t phase = 0;
@@ -260,21 +349,28 @@ __global__ void __launch_bounds__(TC_THREADS, 3) join_tc_kernel(BuildState s, ui
         const bool samp = sampled_node(n);
         for (uint32_t j0 = 0; j0 < a && !aborted; j0 += TC_N) {
             const uint32_t j1 = min(a, j0 + TC_N);
-            stage_rows(s, sh, sh.bbuf, j0, min(U, j0 + TC_M) - j0, warp, lane);
+            stage_rows<PREC>(s, sh, sh.bbuf, j0, min(U, j0 + TC_M) - j0, warp, lane);
             for (uint32_t u0 = 0; u0 < U; u0 += TC_M) {
                 const uint32_t u1 = min(U, u0 + TC_M);
                 if (!(u1 > max(u0, a) || (u0 < a && u0 + 1 < j1))) continue;   // no pair needed in this tile
                 const bool same = u0 == j0;
-                if (!same) stage_rows(s, sh, sh.abuf, u0, u1 - u0, warp, lane);
+                if (!same) stage_rows<PREC>(s, sh, sh.abuf, u0, u1 - u0, warp, lane);
                 tc::fence_before_sync();
                 __syncthreads();
                 if (tid == 0) {
                     tc::fence_after_sync();
-                    const uint32_t idesc = tc::idesc_bf16_f32(TC_M, TC_N);
                     const uint32_t aa = tc::smem_addr(same ? sh.bbuf : sh.abuf), ba = tc::smem_addr(sh.bbuf);
-                    for (uint32_t kk = 0; kk < Dp / 16; ++kk)
-                        tc::mma_bf16(tmem, tc::smem_desc(aa + kk * 256, 128, Dp * 16),
-                                     tc::smem_desc(ba + kk * 256, 128, Dp * 16), idesc, kk > 0);
+                    if constexpr (PREC == 1) {   // K = 32 bytes per step, rows of Dp bytes
+                        const uint32_t idesc = tc::idesc_e4m3_f32(TC_M, TC_N);
+                        for (uint32_t kk = 0; kk < Dp / 32; ++kk)
+                            tc::mma_e4m3(tmem, tc::smem_desc(aa + kk * 256, 128, Dp * 8),
+                                         tc::smem_desc(ba + kk * 256, 128, Dp * 8), idesc, kk > 0);
+                    } else {
+                        const uint32_t idesc = tc::idesc_bf16_f32(TC_M, TC_N);
+                        for (uint32_t kk = 0; kk < Dp / 16; ++kk)
+                            tc::mma_bf16(tmem, tc::smem_desc(aa + kk * 256, 128, Dp * 16),
+                                         tc::smem_desc(ba + kk * 256, 128, Dp * 16), idesc, kk > 0);
+                    }
                     tc::mma_commit(&mbar);
                 }
                 const bool ok = tc::mbar_wait(&mbar, phase, TC_WAIT_CYCLES);
@@ -293,6 +389,7 @@ __global__ void __launch_bounds__(TC_THREADS, 3) join_tc_kernel(BuildState s, ui
                 const bool unew = u < a;
                 const float hu = uval ? sh.ht[u] : 0.f, cu = uval ? sh.cc[u] : 0.f, nuu = uval ? sh.nu[u] : 0.f;
                 const float radu = uval ? sh.rad[u] : -FLT_MAX;
+                const float su = (PREC == 1 && uval) ? sh.scl[u] : 1.f, ru = (PREC == 1 && uval) ? sh.rel[u] : 0.f;
                 const float qn = s_qn;
                 unsigned pmask[2] = {0u, 0u};
                 for (int part = 0; part < 2; ++part) {
@@ -308,8 +405,14 @@ __global__ void __launch_bounds__(TC_THREADS, 3) join_tc_kernel(BuildState s, ui
                         const bool need = uval && idj != NO_ID && (!unew || (j > u && idj != idu));
                         if (need) {
                             ++comps;
-                            const Approx ap = approx_dist(metric, v[c], hu, sh.ht[j], cu, sh.cc[j], nuu, sh.nu[j],
-                                                          qn, et, gam);
+                            float gv = v[c], etp = et;
+                            if constexpr (PREC == 1) {   // the scales, and this pair's relative error
+                                gv = gv * su * sh.scl[j];
+                                const float rj = sh.rel[j];
+                                etp = ru + rj + ru * rj + g8 * (1.f + ru) * (1.f + rj);
+                            }
+                            const Approx ap = approx_dist(metric, gv, hu, sh.ht[j], cu, sh.cc[j], nuu, sh.nu[j],
+                                                          qn, etp, gam);
                             if (!(ap.d - ap.e > fmaxf(radu, sh.rad[j]))) pm |= 1u << c;
                         }
                     }
@@ -333,8 +436,14 @@ __global__ void __launch_bounds__(TC_THREADS, 3) join_tc_kernel(BuildState s, ui
                                 float g = 0.f;
 #pragma unroll
                                 for (int k = 0; k < 32; ++k) if (k == c) g = v[k];
+                                float etp = et;
+                                if constexpr (PREC == 1) {
+                                    g = g * su * sh.scl[j];
+                                    const float rj = sh.rel[j];
+                                    etp = ru + rj + ru * rj + g8 * (1.f + ru) * (1.f + rj);
+                                }
                                 const Approx ap = approx_dist(metric, g, hu, sh.ht[j], cu, sh.cc[j], nuu, sh.nu[j],
-                                                              qn, et, gam);
+                                                              qn, etp, gam);
                                 apd = ap.d;
                                 ape = ap.e;
                                 ia = idu;
@@ -515,14 +624,16 @@ __global__ void join_bounds_kernel(const uint64_t *pre, uint32_t N, uint64_t sla
     }
 }
 
-size_t join_tc_smem(const BuildState &s) {
+size_t join_tc_smem(const BuildState &s, int prec) {
     const size_t Umax = (size_t)s.NEWCAP + s.OLDCAP;
-    return 2 * (size_t)TC_M * s.D.ld * 2 + (size_t)s.D.ld * 4 + Umax * 4 * 5;
+    return 2 * (size_t)TC_M * s.D.ld * (prec ? 1 : 2) + (size_t)s.D.ld * 4 + Umax * 4 * 7;
 }
 
 }  // namespace
 
-bool join_tc_supported(const BuildState &s) { return s.D.ld % 16 == 0 && join_tc_smem(s) <= 200 * 1024; }
+bool join_tc_supported(const BuildState &s, int prec) {
+    return s.D.ld % (prec ? 32 : 16) == 0 && join_tc_smem(s, prec) <= 200 * 1024;
+}
 
 uint64_t join_tc_node_max(const BuildState &s) {
     return (uint64_t)s.NEWCAP * (s.NEWCAP - 1) / 2 + (uint64_t)s.NEWCAP * s.OLDCAP;
@@ -540,18 +651,19 @@ cudaError_t join_tc_bounds(cudaStream_t st, const uint64_t *pre, uint32_t N, uin
 }
 
 cudaError_t launch_join_tc(int num_sms, int grid_insert, cudaStream_t st, const BuildState &s, JoinQueue jq,
-                           uint32_t round) {
-    size_t smem = join_tc_smem(s);
+                           uint32_t round, int prec) {
+    auto kern = prec ? join_tc_kernel<1> : join_tc_kernel<0>;
+    size_t smem = join_tc_smem(s, prec);
     if (smem < TC_MIN_SMEM) smem = TC_MIN_SMEM;
-    cudaError_t e = cudaFuncSetAttribute(join_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(join_tc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                              (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
     // CTAs per SM from the kernel's registers and shared memory (at most
     // JOIN_TC_MAX_CTAS_PER_SM, which bounds the TMEM columns in use per SM).
     cudaFuncAttributes fa{};
-    if ((e = cudaFuncGetAttributes(&fa, join_tc_kernel)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&fa, kern)) != cudaSuccess) return e;
     int dev = 0, smem_sm = 0, smem_rsv = 0, regs_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
@@ -565,7 +677,7 @@ cudaError_t launch_join_tc(int num_sms, int grid_insert, cudaStream_t st, const 
     if (occ < 1) return cudaErrorInvalidConfiguration;
     cudaMemsetAsync(jq.tail, 0, 8, st);
     cudaMemsetAsync(jq.work, 0, 4, st);
-    join_tc_kernel<<<num_sms * occ, TC_THREADS, smem, st>>>(s, s.NEWCAP + s.OLDCAP, jq, round);
+    kern<<<num_sms * occ, TC_THREADS, smem, st>>>(s, s.NEWCAP + s.OLDCAP, jq, round);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     cudaFuncSetAttribute(join_insert_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                          (int)cudaSharedmemCarveoutMaxL1);

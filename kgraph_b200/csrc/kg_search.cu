@@ -461,9 +461,13 @@ __global__ void __launch_bounds__(256, MB) search_kernel(SearchArgs a) {
                     }
                     __syncwarp();
                     n_adj += endM - beginM;
-                    // kgraph.cpp:495-513, in pieces that stay inside one 32-entry chunk
+                    // kgraph.cpp:495-513.  A batch of at most 32 neighbours is one unit (lane j
+                    // holds neighbour beginM + j, gathered from the window, which is reloaded
+                    // when it does not hold the whole batch); a longer batch (S > 32) goes in
+                    // pieces that stay inside one 32-entry chunk.
+                    const bool whole = endM - beginM <= 32;   // warp-uniform
                     for (uint32_t p0 = beginM; p0 < endM;) {
-                        if (p0 < wlo || p0 >= whi) {   // load the window that starts at p0
+                        if (whole ? (p0 < wlo || endM > whi) : (p0 < wlo || p0 >= whi)) {   // load the window at p0
                             wlo = p0;
                             whi = min(p0 + 128u, eM);
 #pragma unroll
@@ -484,15 +488,39 @@ __global__ void __launch_bounds__(256, MB) search_kernel(SearchArgs a) {
                                 if (wuv[c]) wuv[c] = !((__ldcg(vis + (wid[c] >> 5)) >> (wid[c] & 31)) & 1u);
                         }
                         const uint32_t c = (p0 - wlo) >> 5;
-                        const uint32_t cbase = wlo + 32 * c;
-                        const uint32_t p1 = min(endM, cbase + 32);
-                        const uint32_t lo = p0 - cbase, hi = p1 - cbase;
-                        uint32_t id = 0;
-                        bool uv = false;
+                        uint32_t id = 0, p1;
+                        bool cand;
+                        if (whole) {
+                            // the batch spans window chunks c and c + 1 at most
+                            uint32_t idA = 0, idB = 0;
+                            bool uvA = false, uvB = false;
 #pragma unroll
-                        for (int cc = 0; cc < 4; ++cc)
-                            if ((uint32_t)cc == c) { id = wid[cc]; uv = wuv[cc]; }
-                        const bool cand = uv && (uint32_t)lane >= lo && (uint32_t)lane < hi;
+                            for (int cc = 0; cc < 4; ++cc) {
+                                if ((uint32_t)cc == c) { idA = wid[cc]; uvA = wuv[cc]; }
+                                if ((uint32_t)cc == c + 1) { idB = wid[cc]; uvB = wuv[cc]; }
+                            }
+                            const uint32_t pos = p0 - wlo + lane;   // window position of this lane's neighbour
+                            const int src = (int)(pos & 31);
+                            const uint32_t ia = __shfl_sync(FULL, idA, src), ib = __shfl_sync(FULL, idB, src);
+                            const bool ua = __shfl_sync(FULL, uvA, src), ub = __shfl_sync(FULL, uvB, src);
+                            const bool second = (pos >> 5) != c;
+                            id = second ? ib : ia;
+                            const bool uv = (uint32_t)lane < endM - p0 && (second ? ub : ua);
+                            // an id in both chunks: its first position only, as the reference's
+                            // in-order loop marks it visited there (kgraph.cpp:497-498)
+                            const unsigned same = __match_any_sync(FULL, uv ? id : 0xFFFFFFFFu);
+                            cand = uv && (__ffs(same) - 1) == lane;
+                            p1 = endM;
+                        } else {
+                            const uint32_t cbase = wlo + 32 * c;
+                            p1 = min(endM, cbase + 32);
+                            const uint32_t lo = p0 - cbase, hi = p1 - cbase;
+                            bool uv = false;
+#pragma unroll
+                            for (int cc = 0; cc < 4; ++cc)
+                                if ((uint32_t)cc == c) { id = wid[cc]; uv = wuv[cc]; }
+                            cand = uv && (uint32_t)lane >= lo && (uint32_t)lane < hi;
+                        }
                         const unsigned cm = __ballot_sync(FULL, cand);
                         // L2 prefetch of the rows the next PF batches of this entry will
                         // read (unvisited window ids), behind this batch's loads

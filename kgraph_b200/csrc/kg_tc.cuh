@@ -41,6 +41,19 @@ __host__ __device__ constexpr uint32_t idesc_bf16_f32(uint32_t M, uint32_t N) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
 }
 
+// kind::f8f6f4 instruction descriptor: E4M3 x E4M3 (format code 0 for both)
+// -> FP32, both operands K-major.  Same bit layout as kind::f16.
+__host__ __device__ constexpr uint32_t idesc_e4m3_f32(uint32_t M, uint32_t N) {
+    return (1u << 4) | ((N >> 3) << 17) | ((M >> 4) << 24);
+}
+
+// Byte offset of (row r, byte k) in a K-major core-matrix tile whose rows are
+// Kb bytes (8-bit elements: byte k is element k).  Same layout as kmajor_off in
+// bytes: 8 rows x 16 bytes per core matrix, LBO = 128, SBO = Kb * 8.
+__device__ __forceinline__ uint32_t kmajor_off8(uint32_t r, uint32_t k, uint32_t Kb) {
+    return (r >> 3) * (Kb * 8) + (k >> 4) * 128 + (r & 7) * 16 + (k & 15);
+}
+
 __device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -68,6 +81,19 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// One thread: D[tmem] (+)= A[smem] * B[smem]^T for one K=32 step of E4M3
+// operands (32 bytes of each row: the same 256 bytes of the K-major tile as one
+// BF16 step).
+__device__ __forceinline__ void mma_e4m3(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
         : "memory");
 }

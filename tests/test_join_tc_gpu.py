@@ -1,4 +1,4 @@
-"""Tensor-core local join (tcgen05, BF16 tiles + FP32 recheck), through the C-ABI.
+"""Tensor-core local join (tcgen05, BF16 or FP8 E4M3 tiles + FP32 recheck), through the C-ABI.
 
 The BF16 Gram block only decides which pairs can be skipped; every pair that
 may pass the reference's radius test is recomputed with the canonical FP32
@@ -25,12 +25,22 @@ CASES = [("mixture", 12000, 64, "euclidean", dict(K=20, L=40, S=10)),
          ("uniform", 8000, 16, "euclidean", dict(K=25, L=50, S=10))]
 
 
-@pytest.mark.parametrize("kind,n,d,metric,bp", CASES)
-def test_bf16_join_matches_reference_quality(gpu_ctx, kind, n, d, metric, bp):
+FP8_CASES = [("mixture", 12000, 64, "euclidean", dict(K=20, L=40, S=10)),
+             ("mixture", 10000, 128, "euclidean", dict(K=25, L=50, S=10)),
+             ("sphere", 10000, 96, "angular", dict(K=15, L=40, S=8)),
+             ("uniform", 8000, 32, "l2sqr", dict(K=10, L=30, S=8))]
+
+
+@pytest.mark.parametrize("prec,kind,n,d,metric,bp", [("bf16",) + c for c in CASES] + [("fp8",) + c for c in FP8_CASES])
+def test_tc_join_matches_reference_quality(gpu_ctx, prec, kind, n, d, metric, bp):
+    """BF16 tiles, and FP8 E4M3 tiles with a scale per row: the tile only
+    filters, so the graph keeps the reference's quality and every stored
+    distance is canonical; the FP64 check of sampled tile errors never
+    exceeds the margin."""
     from kgraph_b200 import capi
     X = data(kind, n, d, 7 * n + d)
     gpu_ctx.set_data(X, metric)
-    gpu_ctx.set_join_precision("bf16_always")   # the tensor-core filter in every iteration
+    gpu_ctx.set_join_precision(prec + "_always")   # the tensor-core filter in every iteration
     try:
         info = gpu_ctx.build(iterations=30, reverse=0, **bp)
         st = gpu_ctx.join_stats()
@@ -47,7 +57,7 @@ def test_bf16_join_matches_reference_quality(gpu_ctx, kind, n, d, metric, bp):
     r_gpu, r_ref = graph_recall(G, ex_d, K), graph_recall(R, ex_d, K)
     assert abs(r_gpu - r_ref) <= 0.005, (r_gpu, r_ref, info, rinfo, st)
     # the report: the join that ran, its pair count, and a safe margin
-    assert st["mode"] == "bf16" and st["tc_iterations"] == info["iterations"]
+    assert st["mode"] == prec and st["tc_iterations"] == info["iterations"]
     total = n * (n - 1) / 2
     assert abs(st["pairs"] - info["cost"] * total) <= 1e-4 * st["pairs"] + 1
     assert 0 < st["rechecked"] <= st["pairs"]
@@ -84,3 +94,15 @@ def test_join_precision_modes(gpu_ctx):
     # auto runs the CUDA-core join
     gpu_ctx.build(K=10, L=30, S=8, iterations=2)
     assert gpu_ctx.join_stats()["mode"] == "fp32"
+
+
+def test_fp8_join_needs_d_padded_to_32(gpu_ctx):
+    from kgraph_b200 import capi
+    X = data("uniform", 3000, 80, 5)   # rows padded to 80 floats: not a multiple of 32
+    gpu_ctx.set_data(X, "euclidean")
+    gpu_ctx.set_join_precision("fp8_always")
+    try:
+        with pytest.raises(capi.KGError, match="multiple of 32"):
+            gpu_ctx.build(K=10, L=30, S=8, iterations=2)
+    finally:
+        gpu_ctx.set_join_precision("auto")
