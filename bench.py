@@ -591,7 +591,9 @@ def main():
     build_graphs = ctx.build_graph_launches()
     # algorithmic bytes of the build (per iteration and node: the join's list rows, 4 D + 4 bytes each, and
     # one read and one write of the (L+1)-entry pool of 12-byte entries)
-    build_bytes = b_lists * (DIM * 4 + 4) + b_iters * args.n * 2 * (BUILD["L"] + 1) * 12
+    # iterations after the first one that joins no pair change nothing and are counted, not run
+    b_run = sum(1 for r in b_periter if r["ms"] > 0)
+    build_bytes = b_lists * (DIM * 4 + 4) + b_run * args.n * 2 * (BUILD["L"] + 1) * 12
 
     # recall ladder on the GPU-built graph; FP64 ground truth on the GPU
     Xt = torch.as_tensor(X, dtype=torch.float64, device="cuda")
@@ -853,7 +855,8 @@ def main():
                           "first_build_seconds": cold_ms / 1000, "first_build_wall_s": cold_wall,
                           "warm_builds_seconds": [b[0] / 1000 for b in builds],
                           "graph_launches": build_graphs,
-                          "work": {"join_pairs": b_pairs, "join_list_entries": b_lists, "iterations": b_iters},
+                          "work": {"join_pairs": b_pairs, "join_list_entries": b_lists, "iterations": b_iters,
+                                   "iterations_run": b_run},
                           # per NN-descent iteration: device ms, join pairs, list entries, locked insert
                           # attempts and inserts that landed (the median build)
                           "per_iteration": [[round(r["ms"], 3), r["pairs"], r["list_entries"], r["insert_attempts"],
@@ -864,7 +867,7 @@ def main():
                                        "achieved": build_bytes / (build_ms / 1000) / 1e9, "peak": hbm,
                                        "unit": "GB/s", "frac": build_bytes / (build_ms / 1000) / 1e9 / hbm,
                                        "peak_source": peak_source,
-                                       "bytes": "join list entries x (4 D + 4) + iterations x N x 2 (L+1) x 12"}},
+                                       "bytes": "join list entries x (4 D + 4) + iterations run x N x 2 (L+1) x 12"}},
                 "build_parity": parity,
                 # per step: the queries in, and the ids buffer in (the library keeps a caller's entries
                 # beyond each query's result count, as the reference does); ids, distances, counts out

@@ -877,16 +877,35 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
         }
         inf.recall = C ? rs / C : 0.f;
         inf.accuracy = C ? as / C : 0.f;
-        if (g_verbosity > 0) {
+        auto print_iteration = [&]() {
             auto now = std::chrono::steady_clock::now();
             std::cerr << "iteration: " << inf.iterations << " recall: " << inf.recall << " accuracy: " << inf.accuracy
                       << " cost: " << inf.cost << " M: " << inf.M << " delta: " << inf.delta
                       << " time: " << std::chrono::duration<double>(now - t_start).count()
                       << " one-recall: " << (C ? ors / C : 0.f) << " one-ratio: " << (C ? (oa / C) / (oe / C) : 0.f)
                       << std::endl;
-        }
+        };
+        if (g_verbosity > 0) print_iteration();
         if (inf.delta <= params->delta) { inf.stop_condition = 1; stopped = true; break; }
         if (inf.recall >= params->recall) { inf.stop_condition = 2; stopped = true; break; }
+        if (ctx->last_build_iters.back().pairs == 0) {
+            // A join of no pairs lands no insert: the pools stay as they are and
+            // found is clear for every node, so the next update keeps every M
+            // (kgraph.cpp:825-833) and finds no flagged entry below it (the last
+            // update cleared them all), and the next join has no pairs again.
+            // Every remaining iteration of the reference repeats this one, with
+            // the same statistics, and its updates change nothing that reaches
+            // the graph: they are counted, not run.  (Without an iteration cap
+            // the reference would repeat it for ever; the build ends here.)
+            while (params->iterations > 0 && inf.iterations < (uint32_t)params->iterations) {
+                ++inf.iterations;
+                kg_build_iteration idle{};
+                idle.tensor_core = ctx->last_build_iters.back().tensor_core;
+                ctx->last_build_iters.push_back(idle);
+                if (g_verbosity > 0) print_iteration();
+            }
+            break;
+        }
         pending_update = true;   // update (kgraph.cpp:816-883), launched with the next iteration
     }
     // The iteration cap ended the loop: the reference has run the last update

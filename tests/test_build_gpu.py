@@ -154,3 +154,40 @@ def test_build_then_search_python_module(tmp_path):
     k2.load(str(p))
     i2, d2 = k2.search(Q, K=10, P=100, withDistance=True)
     assert (i2 == ids).all() and (bits(d2) == bits(d)).all()
+
+
+def test_idle_iterations_are_counted_not_run(gpu_ctx):
+    """Once an iteration joins no pair, nothing can change any more (no insert
+    lands, found is clear, every M stays, no flagged entry is left below M):
+    the remaining iterations up to the cap are counted with zero work and no
+    device time, and the graph is the one the reference's full loop ends with
+    -- its recall still matches the oracle's 40-iteration build."""
+    X = data("uniform", 6000, 16, 7)
+    bp = dict(K=10, L=30, S=8, iterations=40, reverse=0, delta=-1.0, recall=2.0)
+    gpu_ctx.set_data(X, "euclidean")
+    info = gpu_ctx.build(**bp)
+    its = gpu_ctx.build_iterations()
+    assert info["iterations"] == 40 and len(its) == 40 and info["stop_condition"] == 0
+    z = next(i for i, r in enumerate(its) if r["pairs"] == 0)
+    assert z < 39, "the build must converge well inside 40 iterations for this check"
+    assert all(r["pairs"] > 0 for r in its[:z])
+    for r in its[z + 1:]:
+        assert r["pairs"] == 0 and r["insert_attempts"] == 0 and r["list_entries"] == 0 and r["ms"] == 0.0
+    assert its[z]["insert_attempts"] == 0 and its[z]["inserts_landed"] == 0
+    # one captured-graph launch per iteration run; no final update after the fixed point
+    assert gpu_ctx.build_graph_launches() == z + 1
+    assert gpu_ctx.build_work()[0] == sum(r["pairs"] for r in its)
+    off, ids, dists, M = gpu_ctx.graph()
+    c2 = __import__("kgraph_b200.capi", fromlist=["capi"]).Context(0)
+    c2.set_data(X, "euclidean")
+    ex_i, ex_d = exact_knn(c2, X, 10)
+    c2.close()
+    R, rinfo, rlog = ko.Oracle(X, "euclidean").build(**bp)
+    assert int(rinfo[1]) == 40 and len(rlog) == 40
+    # the oracle runs every iteration: from its first iteration that joins no
+    # pair (the cost stops growing) to the cap, its statistics do not move
+    zi = next(i for i in range(1, 40) if rlog[i, 3] == rlog[i - 1, 3])
+    assert (rlog[zi:, 1:8] == rlog[zi, 1:8]).all()
+    r_gpu = graph_recall(ko.Graph(off, ids, dists, M), ex_d, 10)
+    r_ref = graph_recall(R, ex_d, 10)
+    assert abs(r_gpu - r_ref) <= 0.005, (r_gpu, r_ref, info, rinfo)
