@@ -46,11 +46,13 @@ ROUTER_SEEDS = 3          # starting points per query (the reference requires in
 ROUTER_SEED_CHOICES = [1, 2, 3, 5, 9]   # the operating point search tries each (init < K = 10)
 ROUTER_TRAIN = 200_000    # (query, best node) training pairs
 TARGET = 0.95
-# DRAM read + write of one search launch (10,000 queries, K=10) from ncu
-# captures of the same kernels on the 400k-node version of this workload:
-# the plain walk at P=1000 and the router-seeded walk at P=10.
-SEARCH_DRAM_BYTES_PER_LAUNCH = 22.09e9
-ROUTER_SEARCH_DRAM_BYTES_PER_LAUNCH = 9.081e9
+# DRAM read + write from one-pass ncu captures (dram__bytes_read.sum +
+# dram__bytes_write.sum) of this workload at full size (1M x 128, 10,000
+# queries, K=10), per launch: the plain walk at P=1000, the router-seeded walk
+# at P=5, and the local join summed over the 30 join launches of one warm build.
+SEARCH_DRAM_BYTES_PER_LAUNCH = 114.45e9
+ROUTER_SEARCH_DRAM_BYTES_PER_LAUNCH = 18.00e9
+BUILD_JOIN_DRAM_BYTES = 2124.3e9
 
 
 def _sample(c, n, rng, d):
@@ -866,7 +868,9 @@ def main():
                           "roofline": {"bound": "hbm", "algorithmic_bytes": int(build_bytes),
                                        "achieved": build_bytes / (build_ms / 1000) / 1e9, "peak": hbm,
                                        "unit": "GB/s", "frac": build_bytes / (build_ms / 1000) / 1e9 / hbm,
-                                       "peak_source": peak_source,
+                                       "peak_source": peak_source, "traffic": BUILD_JOIN_DRAM_BYTES,
+                                       "traffic_note": "join_kernel launches of one build; each node's partner "
+                                                       "rows are read once per two of its new entries",
                                        "bytes": "join list entries x (4 D + 4) + iterations run x N x 2 (L+1) x 12"}},
                 "build_parity": parity,
                 # per step: the queries in, and the ids buffer in (the library keeps a caller's entries
