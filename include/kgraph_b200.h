@@ -118,12 +118,23 @@ int kg_search_batch(kg_ctx *ctx, const float *queries, size_t nq, size_t q_strid
  *   regs             registers per thread the kernel is compiled for: 64
  *                    (0 = 64), or 80 (FP32 walk only: fewer spills where
  *                    large pools limit residency anyway)
+ *   compact          1: 8-byte pool entries instead of 12 (the id in the
+ *                    bits N needs, the expansion progress in batches of S in
+ *                    the rest of 31 bits; M read again when an entry is
+ *                    expanded), so more queries fit on an SM where the pool's
+ *                    shared memory limits residency (large P).  Used by the
+ *                    FP32 walk where the graph allows it (S >= 1, every
+ *                    node's min(max(M, params M), degree) <= (2^(31 - id
+ *                    bits) - 1) S); elsewhere the 12-byte entry runs.
+ *                    A new context starts with split 4, warps_per_block 0,
+ *                    prefetch 2, regs 64, compact 1.
  * ms / default_ms / variants are filled by kg_search_autotune. */
 typedef struct {
     unsigned split, warps_per_block, prefetch;
     float ms, default_ms;
     unsigned variants;
     unsigned regs;
+    unsigned compact;
 } kg_search_tuning;
 /* Times every shape on `queries` (a representative sample), checks that all
  * of them return identical ids, distances, counts and costs, and keeps the
@@ -133,9 +144,13 @@ typedef struct {
 int kg_search_autotune(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_bytes,
                        const kg_search_params *params, const uint32_t *K_per_q, const uint32_t *P_per_q,
                        const uint32_t *init_ids, size_t init_ld, kg_search_tuning *best);
-/* Sets / reads the context's search shape (split, warps_per_block, prefetch). */
+/* Sets / reads the context's search shape (split, warps_per_block, prefetch, regs, compact). */
 int kg_set_search_tuning(kg_ctx *ctx, const kg_search_tuning *t);
 int kg_get_search_tuning(kg_ctx *ctx, kg_search_tuning *t);
+/* The shape the last kg_search_batch actually launched: warps_per_block as
+ * chosen (0 when every query went to the tensor-core brute force), compact = 1
+ * only if the compact pool entry ran, ms its device time. */
+int kg_last_search_shape(kg_ctx *ctx, kg_search_tuning *t);
 
 /* Distance filter of the search.  No counterpart in the reference (its walk
  * evaluates every candidate in FP32, kgraph.cpp:495-513).  With BF16 or FP8

@@ -22,7 +22,8 @@ SYMBOLS = [
     "kg_last_search_work", "kg_search_batch_noalloc", "kg_noalloc_scratch_bytes",
     "kg_router_params_default", "kg_router_train", "kg_router_seeds", "kg_router_gradients", "kg_last_router_timing",
     "kg_set_join_precision", "kg_last_join_stats", "kg_last_build_graphs", "kg_search_autotune",
-    "kg_set_search_tuning", "kg_get_search_tuning", "kg_set_search_precision", "kg_last_search_filter",
+    "kg_set_search_tuning", "kg_get_search_tuning", "kg_last_search_shape", "kg_set_search_precision",
+    "kg_last_search_filter",
     "kg_filter_bounds", "kg_router_search", "kg_tc_gemm_check", "kg_tc_assign_check", "kg_last_build_work",
     "kg_last_build_iterations", "kg_set_bruteforce_mode", "kg_last_bruteforce_stats",
 ]
@@ -63,7 +64,7 @@ class JoinStats(C.Structure):
 
 class SearchTuning(C.Structure):
     _fields_ = [("split", C.c_uint), ("warps_per_block", C.c_uint), ("prefetch", C.c_uint), ("ms", C.c_float),
-                ("default_ms", C.c_float), ("variants", C.c_uint), ("regs", C.c_uint)]
+                ("default_ms", C.c_float), ("variants", C.c_uint), ("regs", C.c_uint), ("compact", C.c_uint)]
 
 
 class FilterStats(C.Structure):
@@ -133,6 +134,7 @@ def lib():
                                          C.POINTER(SearchTuning)]
         L.kg_set_search_tuning.argtypes = [vp, C.POINTER(SearchTuning)]
         L.kg_get_search_tuning.argtypes = [vp, C.POINTER(SearchTuning)]
+        L.kg_last_search_shape.argtypes = [vp, C.POINTER(SearchTuning)]
         L.kg_set_search_precision.argtypes = [vp, C.c_int]
         L.kg_last_search_filter.argtypes = [vp, C.POINTER(FilterStats)]
         L.kg_filter_bounds.argtypes = [vp, vp, sz, sz, vp, sz, vp, vp]
@@ -401,14 +403,22 @@ class Context:
                                               _ptr(pq), _ptr(ii), 0 if ii is None else ii.shape[1], C.byref(t)))
         return {f: getattr(t, f) for f, _ in SearchTuning._fields_}
 
-    def set_search_tuning(self, split=4, warps_per_block=0, prefetch=2, regs=64):
-        t = SearchTuning(split, warps_per_block, prefetch, 0.0, 0.0, 0, regs)
+    def set_search_tuning(self, split=4, warps_per_block=0, prefetch=2, regs=64, compact=1):
+        t = SearchTuning(split, warps_per_block, prefetch, 0.0, 0.0, 0, regs, compact)
         self._check(self.L.kg_set_search_tuning(self.h, C.byref(t)))
 
     def search_tuning(self):
         t = SearchTuning()
         self._check(self.L.kg_get_search_tuning(self.h, C.byref(t)))
-        return {"split": t.split, "warps_per_block": t.warps_per_block, "prefetch": t.prefetch, "regs": t.regs}
+        return {"split": t.split, "warps_per_block": t.warps_per_block, "prefetch": t.prefetch, "regs": t.regs,
+                "compact": t.compact}
+
+    def last_search_shape(self):
+        """kg_last_search_shape: the shape the last search launched (compact = 1 if the compact pool ran)."""
+        t = SearchTuning()
+        self._check(self.L.kg_last_search_shape(self.h, C.byref(t)))
+        return {"split": t.split, "warps_per_block": t.warps_per_block, "prefetch": t.prefetch, "regs": t.regs,
+                "compact": t.compact, "ms": t.ms}
 
     def set_search_precision(self, mode):
         """'fp32' (default), 'bf16' or 'fp8': compressed rows that filter the walk's candidates."""

@@ -85,12 +85,19 @@ __global__ void norms_kernel(DataView D, float *norms) {
     }
 }
 
-__global__ void maxdeg_kernel(uint32_t N, const uint64_t *off, uint32_t *out) {
-    uint32_t m = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
-        m = max(m, (uint32_t)(off[i + 1] - off[i]));
-    for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+// out[0] = the largest degree, out[1] = the largest min(M, degree).
+__global__ void maxdeg_kernel(uint32_t N, const uint64_t *off, const uint32_t *M, uint32_t *out) {
+    uint32_t m = 0, mm = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const uint32_t deg = (uint32_t)(off[i + 1] - off[i]);
+        m = max(m, deg);
+        mm = max(mm, min(M[i], deg));
+    }
+    for (int o = 16; o; o >>= 1) {
+        m = max(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+        mm = max(mm, __shfl_xor_sync(0xFFFFFFFFu, mm, o));
+    }
+    if ((threadIdx.x & 31) == 0) { atomicMax(out, m); atomicMax(out + 1, mm); }
 }
 
 // ELL copy of the first W neighbours of every node and its {M, degree}.
@@ -281,11 +288,15 @@ int ensure_search_layout(kg_ctx *ctx) {
     const uint32_t N = ctx->gn;
     cudaError_t e;
     uint32_t *dmax = ctx->counter.as<uint32_t>() + 12;
-    cudaMemsetAsync(dmax, 0, 4, ctx->stream);
-    maxdeg_kernel<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(N, ctx->offsets.as<uint64_t>(), dmax);
-    uint32_t maxdeg = 0;
-    cudaMemcpyAsync(&maxdeg, dmax, 4, cudaMemcpyDeviceToHost, ctx->stream);
+    cudaMemsetAsync(dmax, 0, 8, ctx->stream);
+    maxdeg_kernel<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(N, ctx->offsets.as<uint64_t>(), ctx->Mnode.as<uint32_t>(),
+                                                              dmax);
+    uint32_t hmax[2] = {0, 0};
+    cudaMemcpyAsync(hmax, dmax, 8, cudaMemcpyDeviceToHost, ctx->stream);
     if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "layout");
+    const uint32_t maxdeg = hmax[0];
+    ctx->max_degree = hmax[0];
+    ctx->max_mdeg = hmax[1];
     uint32_t W = std::min<uint32_t>(128, std::max<uint32_t>(32, (maxdeg + 31) / 32 * 32));
     if ((e = ctx->ell.reserve((size_t)N * W * 4 + 4)) != cudaSuccess ||
         (e = ctx->meta.reserve((size_t)N * 8 + 8)) != cudaSuccess)
@@ -378,6 +389,8 @@ int search_locked(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_
         a.ell = ctx->ell.as<uint32_t>();
         a.ell_w = ctx->ell_w;
         a.meta = ctx->meta.as<uint2>();
+        a.compact_ok = compact_pool_ok(ctx, N, params->S, params->M);
+        a.cp_idbits = compact_id_bits(N);
     }
     a.nq = (uint32_t)Q;
     a.q_ld = ld;
@@ -469,6 +482,15 @@ int search_locked(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_
         } else a.out_cost = costs;
     }
 
+    // the filter's compressed rows: before the visited sets are sized, since the kernel
+    // variant (and so its residency) depends on them
+    if (graph && ctx->search_prec != KG_SEARCH_FP32) {
+        int pr = ensure_search_precision(ctx);
+        if (pr != KG_OK) return pr;
+        a.prec = (uint32_t)ctx->search_prec;
+        a.Xc = ctx->Xc.p;
+        a.cmeta = ctx->cmeta.as<float4>();
+    }
     // visited sets: one per resident warp
     a.vwords = ((N + 31) / 32 + 3) / 4 * 4;
     uint32_t slots = search_max_slots(a, sh, ctx->num_sms);
@@ -479,13 +501,6 @@ int search_locked(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_
     a.err = ctx->errw.as<uint32_t>();
     a.work = reinterpret_cast<unsigned long long *>(ctx->counter.as<char>() + 16);
     cudaMemsetAsync(ctx->counter.p, 0, 48, ctx->stream);
-    if (graph && ctx->search_prec != KG_SEARCH_FP32) {
-        int pr = ensure_search_precision(ctx);
-        if (pr != KG_OK) return pr;
-        a.prec = (uint32_t)ctx->search_prec;
-        a.Xc = ctx->Xc.p;
-        a.cmeta = ctx->cmeta.as<float4>();
-    }
 
     // every query a brute-force query (no graph, or P >= N): the tensor-core path where it applies
     bool bf_all = !graph || (!P_per_q && params->P >= N);
@@ -510,6 +525,9 @@ int search_locked(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_
     } else if ((e = launch_search(a, sh, ctx->num_sms, ctx->stream, nullptr)) != cudaSuccess) {
         return cuda_fail(ctx, e, "search launch");
     }
+    ctx->last_shape = sh;   // the shape as launched: its query tile and whether the compact pool ran
+    ctx->last_shape.warps_per_block = use_tc_bf ? 0u : a.warps_per_block;
+    ctx->last_shape.compact = (!use_tc_bf && search_uses_compact(a, sh)) ? 1u : 0u;
     cudaEventRecord(ctx->ev1, ctx->stream);
     unsigned long long bf_h[2] = {0, 0};
     if (use_tc_bf) cudaMemcpyAsync(bf_h, ctx->bf_stats_dev, 16, cudaMemcpyDeviceToHost, ctx->stream);
@@ -563,6 +581,7 @@ SearchShape shape_of(const kg_search_tuning &t) {
     sh.warps_per_block = t.warps_per_block;
     sh.prefetch = t.prefetch;
     sh.regs = t.regs;
+    sh.compact = t.compact;
     return sh;
 }
 }  // namespace
@@ -573,7 +592,7 @@ int kg_set_search_tuning(kg_ctx *ctx, const kg_search_tuning *t) {
     const SearchShape sh = shape_of(*t);
     if (!search_shape_valid(sh) || sh.split == 0)
         return set_error(ctx, KG_E_INVALID, "search tuning: split must be 2, 4 or 8, warps_per_block 0, 1, 2, 4 or "
-                                            "8, prefetch 0 or 2, regs 0, 64 or 80");
+                                            "8, prefetch 0 or 2, regs 0, 64 or 80, compact 0 or 1");
     ctx->search_shape = sh;
     return KG_OK;
 }
@@ -586,6 +605,20 @@ int kg_get_search_tuning(kg_ctx *ctx, kg_search_tuning *t) {
     t->warps_per_block = ctx->search_shape.warps_per_block;
     t->prefetch = ctx->search_shape.prefetch;
     t->regs = ctx->search_shape.regs;
+    t->compact = ctx->search_shape.compact;
+    return KG_OK;
+}
+
+int kg_last_search_shape(kg_ctx *ctx, kg_search_tuning *t) {
+    if (!ctx || !t) return KG_E_INVALID;
+    Lock lk(ctx);
+    *t = kg_search_tuning{};
+    t->split = ctx->last_shape.split;
+    t->warps_per_block = ctx->last_shape.warps_per_block;
+    t->prefetch = ctx->last_shape.prefetch;
+    t->regs = ctx->last_shape.regs;
+    t->compact = ctx->last_shape.compact;
+    t->ms = ctx->last_search_ms;
     return KG_OK;
 }
 
@@ -640,12 +673,21 @@ int kg_search_autotune(kg_ctx *ctx, const float *queries, size_t nq, size_t q_st
     // the 80-register budget only has FP32-walk variants
     const std::vector<uint32_t> budgets =
         ctx->search_prec == KG_SEARCH_FP32 ? std::vector<uint32_t>{64u, 80u} : std::vector<uint32_t>{64u};
+    // the compact pool entry only where the FP32 walk can use it on this graph
+    const uint32_t N = ctx->has_graph ? ctx->gn : ctx->n;
+    bool cp_ok = ctx->search_prec == KG_SEARCH_FP32 && ctx->has_graph;
+    if (cp_ok) {
+        if ((r = ensure_search_layout(ctx)) != KG_OK) return r;
+        cp_ok = compact_pool_ok(ctx, N, params->S, params->M) != 0;
+    }
+    const std::vector<uint32_t> pools = cp_ok ? std::vector<uint32_t>{0u, 1u} : std::vector<uint32_t>{0u};
+    for (uint32_t cp : pools)
     for (uint32_t regs : budgets)
     for (uint32_t split : {2u, 4u, 8u})
         for (uint32_t wpb : {2u, 4u, 8u})
             for (uint32_t pf : {0u, 2u}) {
                 SearchShape sh;
-                sh.split = split; sh.warps_per_block = wpb; sh.prefetch = pf; sh.regs = regs;
+                sh.split = split; sh.warps_per_block = wpb; sh.prefetch = pf; sh.regs = regs; sh.compact = cp;
                 float ms = 0.f;
                 if ((r = run(sh, &ms)) != KG_OK) return r;
                 ++variants;
@@ -664,6 +706,7 @@ int kg_search_autotune(kg_ctx *ctx, const float *queries, size_t nq, size_t q_st
         best->warps_per_block = top.warps_per_block;
         best->prefetch = top.prefetch;
         best->regs = top.regs;
+        best->compact = top.compact;
         best->ms = top_ms;
         best->default_ms = def_ms;
         best->variants = variants;

@@ -1,5 +1,6 @@
 // Library context: one GPU, one stream, the dataset and the graph in HBM.
 #pragma once
+#include <algorithm>
 #include <cstdint>
 #include <mutex>
 #include <string>
@@ -76,7 +77,9 @@ struct kg_ctx {
     // search-side copy of the graph: ELL rows of the first ell_w neighbours + {M, degree}
     kgb::DevBuf ell, meta;
     uint32_t ell_w = 0;
+    uint32_t max_degree = 0, max_mdeg = 0;   // largest degree and largest min(M, degree) of the graph
     kgb::SearchShape search_shape;   // launch shape of the search kernel (kg_search_autotune)
+    kgb::SearchShape last_shape;     // the shape the last kg_search_batch launched (kg_last_search_shape)
     uint64_t layout_version = ~0ull;
 
     // scratch
@@ -116,6 +119,22 @@ int search_locked(kg_ctx *ctx, const float *queries, size_t nq, size_t q_stride_
                   const kg_search_params *params, const uint32_t *K_per_q, const uint32_t *P_per_q, size_t out_ld,
                   uint32_t *ids, float *dists, uint32_t *counts, float *costs, const SearchShape &sh,
                   const uint32_t *init_dev, size_t init_ld);
+// The id bits of a compact pool word for N nodes (ids 0 .. N-1).
+inline uint32_t compact_id_bits(uint32_t N) {
+    uint32_t b = 1;
+    while (b < 31 && (N - 1) >> b) ++b;
+    return b;
+}
+// Whether the search may use the compact 8-byte pool entry on the current
+// graph (its search layout built): S >= 1 and every node's expansion,
+// min(max(M, Mp), degree), at most 2^(31 - id bits) - 1 batches of S.
+inline uint32_t compact_pool_ok(const kg_ctx *ctx, uint32_t N, uint32_t S, uint32_t Mp) {
+    if (ctx->layout_version != ctx->graph_version || S == 0 || N == 0) return 0;
+    const uint32_t pbits = 31 - compact_id_bits(N);
+    // min(max(M_i, Mp), deg_i) <= max(min(M_i, deg_i), min(Mp, deg_i))
+    const uint64_t em = std::max<uint64_t>(ctx->max_mdeg, std::min<uint64_t>(Mp, ctx->max_degree));
+    return pbits >= 1 && em <= ((1ull << pbits) - 1) * S ? 1u : 0u;
+}
 // Builds the compressed rows of ctx->search_prec if the dataset changed since.
 int ensure_search_precision(kg_ctx *ctx);
 // Exact top-K brute force of `nq` dataset rows (LinearSearch, kgraph.cpp:212-229)

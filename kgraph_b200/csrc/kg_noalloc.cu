@@ -118,6 +118,8 @@ extern "C" int kg_search_batch_noalloc(kg_ctx *ctx, const float *queries, size_t
         a.ell = ctx->ell.as<uint32_t>();
         a.ell_w = ctx->ell_w;
         a.meta = ctx->meta.as<uint2>();
+        a.compact_ok = compact_pool_ok(ctx, N, params->S, params->M);
+        a.cp_idbits = compact_id_bits(N);
     }
     if (graph && ctx->search_prec != KG_SEARCH_FP32 && ctx->prec_built == ctx->search_prec &&
         ctx->prec_data_version == ctx->data_version) {

@@ -6,7 +6,12 @@
 // The warp keeps the query vector and its candidate pool (K+P+1 entries:
 // dist, id|flag, m|M<<16 -- the reference's NeighborX) in shared memory, and
 // a private N-bit visited set in global memory (the reference's
-// dynamic_bitset, kgraph.cpp:438).
+// dynamic_bitset, kgraph.cpp:438).  The compact pool (CP) packs an entry
+// into 8 bytes -- dist, and id (the bits N needs) | expansion progress m/S
+// (the remaining bits up to 31) | flag -- and reads M again from the node's
+// {M, degree} when the entry is expanded, together with its first adjacency
+// window: a third fewer bytes per entry, so more queries fit on an SM where
+// the pool limits residency.
 //
 // Exactness.  The walk is the reference's, step for step: the same P seeds
 // for every query (host mt19937(seed) + GenRandom, kgraph.cpp:444-453), the
@@ -29,17 +34,18 @@ namespace kgb {
 
 namespace {
 
-struct PoolAcc {   // accessor for gnu_sort over the smem pool triples
+template <bool HM>
+struct PoolAcc {   // accessor for gnu_sort over the smem pool (with the m|M words when HM)
     float *d; uint32_t *i; uint32_t *m;
     struct Rec { float d; uint32_t i, m; };
     __device__ float key(int x) const { return d[x]; }
     __device__ void swap(int x, int y) const {
         float td = d[x]; d[x] = d[y]; d[y] = td;
         uint32_t ti = i[x]; i[x] = i[y]; i[y] = ti;
-        uint32_t tm = m[x]; m[x] = m[y]; m[y] = tm;
+        if constexpr (HM) { uint32_t tm = m[x]; m[x] = m[y]; m[y] = tm; }
     }
-    __device__ Rec get(int x) const { return Rec{d[x], i[x], m[x]}; }
-    __device__ void put(int x, Rec r) const { d[x] = r.d; i[x] = r.i; m[x] = r.m; }
+    __device__ Rec get(int x) const { return Rec{d[x], i[x], HM ? m[x] : 0u}; }
+    __device__ void put(int x, Rec r) const { d[x] = r.d; i[x] = r.i; if constexpr (HM) m[x] = r.m; }
     __device__ float rkey(Rec r) const { return r.d; }
 };
 
@@ -55,13 +61,15 @@ struct WarpSmem {
     uint32_t *cM;      // 32    batch actual_M
 };
 
+template <int CP>
 __device__ __forceinline__ WarpSmem carve(char *base, const SearchArgs &a) {
     WarpSmem s;
     char *p = base;
     s.q = reinterpret_cast<float *>(p); p += sizeof(float) * a.D.ld;
     s.pd = reinterpret_cast<float *>(p); p += sizeof(float) * a.cap;
     s.pid = reinterpret_cast<uint32_t *>(p); p += sizeof(uint32_t) * a.cap;
-    s.pm = reinterpret_cast<uint32_t *>(p); p += sizeof(uint32_t) * a.cap;
+    s.pm = nullptr;
+    if constexpr (!CP) { s.pm = reinterpret_cast<uint32_t *>(p); p += sizeof(uint32_t) * a.cap; }
     s.rd = reinterpret_cast<float *>(p); p += sizeof(float) * a.rcap;
     s.rid = reinterpret_cast<uint32_t *>(p); p += sizeof(uint32_t) * a.rcap;
     s.cd = reinterpret_cast<float *>(p); p += sizeof(float) * 32;
@@ -299,14 +307,18 @@ __device__ __forceinline__ void prefetch_crow(const SearchArgs &a, uint32_t id) 
 // compressed rows (1 BF16, 2 FP8) that filter candidates once the pool is full.
 // MB: resident blocks of 256 threads per SM the register allocation is sized
 // for (4: 64 registers per thread; 3: 80, fewer spills for large pools, whose
-// shared memory limits residency anyway).
-template <int G, int PF, int PREC, int MB>
+// shared memory limits residency anyway).  CP: the compact 8-byte pool entry
+// (the host selects it only when every node's expansion fits the progress
+// field: a.cp_idbits id bits, 31 - a.cp_idbits progress bits).
+template <int G, int PF, int PREC, int MB, int CP>
 __global__ void __launch_bounds__(256, MB) search_kernel(SearchArgs a) {
     extern __shared__ __align__(16) char smem[];
+    const uint32_t IDM = CP ? (1u << a.cp_idbits) - 1u : ID_MASK;   // the id bits of a pool word
+    const uint32_t PMASK = CP ? ID_MASK >> a.cp_idbits : 0u;        // the progress bits, shifted down
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const uint32_t slot = blockIdx.x * a.warps_per_block + wib;
-    WarpSmem s = carve(smem + (size_t)wib * a.warp_smem_bytes, a);
+    WarpSmem s = carve<CP>(smem + (size_t)wib * a.warp_smem_bytes, a);
     uint32_t *vis = a.visited + (size_t)slot * a.vwords;
     const uint32_t N = a.D.n;
 
@@ -400,19 +412,21 @@ __global__ void __launch_bounds__(256, MB) search_kernel(SearchArgs a) {
                 }
                 if (j < L && !bad) {
                     atomicOr(vis + (id >> 5), 1u << (id & 31));
-                    s.pm[j] = actual_M(a, a.Mp, id) << 16;
+                    if constexpr (!CP) s.pm[j] = actual_M(a, a.Mp, id) << 16;
                 }
                 __syncwarp();
                 uint32_t cnt = min(32u, L - base);
                 if (j < L) s.cid[lane] = bad ? 0u : id;
                 __syncwarp();
                 batch_dist<G>(a, s, qn, cnt, lane);
-                if (j < L) { s.pd[j] = s.cd[lane]; s.pid[j] = id | FLAG_BIT; }
+                // an out-of-range starting point (the error is raised above) enters as id 0,
+                // unflagged: it is never expanded, so no adjacency row is read for it
+                if (j < L) { s.pd[j] = s.cd[lane]; s.pid[j] = bad ? 0u : (id | FLAG_BIT); }
                 __syncwarp();
             }
             // kgraph.cpp:476: std::sort by dist (GNU introsort order for ties)
             if (lane == 0) {
-                PoolAcc acc{s.pd, s.pid, s.pm};
+                PoolAcc<!CP> acc{s.pd, s.pid, s.pm};
                 gnu_sort(acc, 0, (int)L);
             }
             __syncwarp();
@@ -436,12 +450,30 @@ __global__ void __launch_bounds__(256, MB) search_kernel(SearchArgs a) {
             while (true) {
                 k = warp_next_flagged(s.pid, k, L, lane);
                 if (k >= L) break;
-                const uint32_t node = s.pid[k] & ID_MASK;
-                const uint32_t mM0 = s.pm[k];
-                const uint32_t eM = mM0 >> 16;
-                uint32_t m = mM0 & 0xFFFFu;
-                uint32_t wlo = 0, whi = 0;   // loaded window [wlo, whi)
+                const uint32_t pk = s.pid[k];
+                const uint32_t node = pk & IDM;
+                uint32_t eM, m, bq = 0;
                 uint32_t wid[4];
+                bool pre = false;   // CP: wid holds the ELL ids of the window at m
+                if constexpr (CP) {
+                    // the node's {M, degree} and its first window's ELL ids in flight together
+                    bq = (pk >> a.cp_idbits) & PMASK;
+                    m = bq * S;
+                    if (a.ell) {
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) {
+                            const uint32_t p = m + 32 * c + lane;
+                            wid[c] = p < a.ell_w ? a.ell[(size_t)node * a.ell_w + p] : 0xFFFFFFFFu;
+                        }
+                        pre = true;
+                    }
+                    eM = actual_M(a, a.Mp, node);
+                } else {
+                    const uint32_t mM0 = s.pm[k];
+                    eM = mM0 >> 16;
+                    m = mM0 & 0xFFFFu;
+                }
+                uint32_t wlo = 0, whi = 0;   // loaded window [wlo, whi)
                 bool wuv[4];
                 bool moved = false;
                 while (true) {
@@ -456,8 +488,12 @@ __global__ void __launch_bounds__(256, MB) search_kernel(SearchArgs a) {
                     const bool done = endM > eM;
                     if (done) endM = eM;
                     if (lane == 0) {
-                        if (done) s.pid[k] = s.pid[k] & ID_MASK;
-                        s.pm[k] = (endM & 0xFFFFu) | (eM << 16);
+                        if constexpr (CP) {   // progress in batches of S: endM = (bq + 1) S unless done
+                            s.pid[k] = done ? node : (node | FLAG_BIT | ((bq + 1) << a.cp_idbits));
+                        } else {
+                            if (done) s.pid[k] = s.pid[k] & ID_MASK;
+                            s.pm[k] = (endM & 0xFFFFu) | (eM << 16);
+                        }
                     }
                     __syncwarp();
                     n_adj += endM - beginM;
@@ -474,7 +510,8 @@ __global__ void __launch_bounds__(256, MB) search_kernel(SearchArgs a) {
                             for (int c = 0; c < 4; ++c) {
                                 const uint32_t p = wlo + 32 * c + lane;
                                 const bool act = p < whi;
-                                uint32_t id = act ? neighbour(a, node, p) : 0xFFFFFFFFu;
+                                uint32_t id = 0xFFFFFFFFu;
+                                if (act) id = (CP && pre && p < a.ell_w) ? wid[c] : neighbour(a, node, p);
                                 const bool bad = act && id >= N;
                                 if (__any_sync(FULL, bad)) { if (lane == 0) raise_error(a.err, ERR_BAD_ID); }
                                 const bool ok = act && !bad;
@@ -486,6 +523,7 @@ __global__ void __launch_bounds__(256, MB) search_kernel(SearchArgs a) {
 #pragma unroll
                             for (int c = 0; c < 4; ++c)   // first occurrences not yet visited
                                 if (wuv[c]) wuv[c] = !((__ldcg(vis + (wid[c] >> 5)) >> (wid[c] & 31)) & 1u);
+                            pre = false;
                         }
                         const uint32_t c = (p0 - wlo) >> 5;
                         uint32_t id = 0, p1;
@@ -552,12 +590,12 @@ __global__ void __launch_bounds__(256, MB) search_kernel(SearchArgs a) {
                             n_apx += __popc(nm);
                             n_skip += __popc(nm & ~km);
                             if (km) {
-                                const uint32_t aM = keep ? actual_M(a, a.Mp, id) : 0u;
+                                const uint32_t aM = (!CP && keep) ? actual_M(a, a.Mp, id) : 0u;
                                 const float dd = warp_cand_dist<G>(a, s.q, qn, s.cid, km, keep, id, lane);
                                 const unsigned im = __ballot_sync(FULL, keep && dd < worst);
                                 if (im) {
                                     uint32_t mr;
-                                    L = warp_batch_insert(s.pd, s.pid, s.pm, L, cap, im, dd, id | FLAG_BIT, aM << 16,
+                                    L = warp_batch_insert(s.pd, s.pid, CP ? nullptr : s.pm, L, cap, im, dd, id | FLAG_BIT, aM << 16,
                                                           &mr, lane);
                                     if (mr <= k) moved = true;
                                     if (mr < k) k = mr;
@@ -571,7 +609,7 @@ __global__ void __launch_bounds__(256, MB) search_kernel(SearchArgs a) {
                             if (cand) {
                                 const uint32_t bit = 1u << (id & 31);
                                 isnew = !(atomicOr(vis + (id >> 5), bit) & bit);
-                                aM = actual_M(a, a.Mp, id);
+                                if constexpr (!CP) aM = actual_M(a, a.Mp, id);
                             }
                             const float dd = warp_cand_dist<G>(a, s.q, qn, s.cid, cm, cand, id, lane);
                             const unsigned nm = __ballot_sync(FULL, isnew);
@@ -584,7 +622,7 @@ __global__ void __launch_bounds__(256, MB) search_kernel(SearchArgs a) {
                                 L == cap - 1 ? __ballot_sync(FULL, isnew && dd < s.pd[L - 1]) : nm;
                             if (im) {
                                 uint32_t mr;   // new entries: flag set, m = 0, M = actual_M
-                                L = warp_batch_insert(s.pd, s.pid, s.pm, L, cap, im, dd, id | FLAG_BIT, aM << 16,
+                                L = warp_batch_insert(s.pd, s.pid, CP ? nullptr : s.pm, L, cap, im, dd, id | FLAG_BIT, aM << 16,
                                                       &mr, lane);
                                 if (mr <= k) moved = true;   // the expanded entry is no longer at k
                                 if (mr < k) k = mr;
@@ -593,19 +631,21 @@ __global__ void __launch_bounds__(256, MB) search_kernel(SearchArgs a) {
                         p0 = p1;
                     }
                     m = endM;
+                    ++bq;
                     if (done || moved) break;   // the loop head picks the reference's next k
                 }
                 if (k >= L) break;
             }
             if (L > K) L = K;   // kgraph.cpp:515
             if (!have_results) {
-                for (uint32_t j = lane; j < L; j += 32) { s.rd[j] = s.pd[j]; s.rid[j] = s.pid[j]; }
+                for (uint32_t j = lane; j < L; j += 32) { s.rd[j] = s.pd[j]; s.rid[j] = s.pid[j] & (IDM | FLAG_BIT); }
                 rn = L;
                 have_results = true;
                 __syncwarp();
             } else {   // kgraph.cpp:521-528
                 for (uint32_t l = 0; l < L; ++l) {
-                    uint32_t r = warp_update_knn(s.rd, s.rid, (uint32_t *)nullptr, rn, s.pd[l], s.pid[l], 0u, lane);
+                    uint32_t r = warp_update_knn(s.rd, s.rid, (uint32_t *)nullptr, rn, s.pd[l], s.pid[l] & (IDM | FLAG_BIT),
+                                                 0u, lane);
                     if (r < rn + 1 && rn + 1 < K + 1) ++rn;
                 }
             }
@@ -678,30 +718,34 @@ cudaError_t launch_filter_bounds(const SearchArgs &a, const uint32_t *ids, uint3
     return cudaGetLastError();
 }
 
-size_t search_warp_smem_bytes(uint32_t ld, uint32_t cap, uint32_t rcap) {
-    size_t b = sizeof(float) * ld + 12ull * cap + 8ull * rcap + 12ull * 32;
+size_t search_warp_smem_bytes(uint32_t ld, uint32_t cap, uint32_t rcap, bool compact) {
+    size_t b = sizeof(float) * ld + (compact ? 8ull : 12ull) * cap + 8ull * rcap + 12ull * 32;
     return (b + 15) & ~size_t(15);
 }
 
 namespace {
 
 using SearchFn = void (*)(SearchArgs);
-template <int PREC, int MB>
+template <int PREC, int MB, int CP>
 SearchFn search_fn_prec(uint32_t split, bool pf) {
     switch (split) {
-        case 2: return pf ? search_kernel<2, 2, PREC, MB> : search_kernel<2, 0, PREC, MB>;
-        case 8: return pf ? search_kernel<8, 2, PREC, MB> : search_kernel<8, 0, PREC, MB>;
-        default: return pf ? search_kernel<4, 2, PREC, MB> : search_kernel<4, 0, PREC, MB>;
+        case 2: return pf ? search_kernel<2, 2, PREC, MB, CP> : search_kernel<2, 0, PREC, MB, CP>;
+        case 8: return pf ? search_kernel<8, 2, PREC, MB, CP> : search_kernel<8, 0, PREC, MB, CP>;
+        default: return pf ? search_kernel<4, 2, PREC, MB, CP> : search_kernel<4, 0, PREC, MB, CP>;
     }
 }
-// The compiled (D-split, prefetch, filter precision, register budget) variants;
-// the 80-register budget exists for the FP32 walk.
-SearchFn search_fn(uint32_t split, uint32_t prefetch, uint32_t prec, uint32_t regs) {
+// The compiled (D-split, prefetch, filter precision, register budget, pool
+// entry) variants; the 80-register budget and the compact pool exist for the
+// FP32 walk.
+SearchFn search_fn(uint32_t split, uint32_t prefetch, uint32_t prec, uint32_t regs, bool compact) {
     const bool pf = prefetch > 0;
-    if (prec == 1) return search_fn_prec<1, 4>(split, pf);
-    if (prec == 2) return search_fn_prec<2, 4>(split, pf);
-    return regs == 80 ? search_fn_prec<0, 3>(split, pf) : search_fn_prec<0, 4>(split, pf);
+    if (prec == 1) return search_fn_prec<1, 4, 0>(split, pf);
+    if (prec == 2) return search_fn_prec<2, 4, 0>(split, pf);
+    if (compact) return regs == 80 ? search_fn_prec<0, 3, 1>(split, pf) : search_fn_prec<0, 4, 1>(split, pf);
+    return regs == 80 ? search_fn_prec<0, 3, 0>(split, pf) : search_fn_prec<0, 4, 0>(split, pf);
 }
+// The compact pool runs where the shape asks for it and the graph allows it.
+bool use_compact(const SearchArgs &a, const SearchShape &sh) { return search_uses_compact(a, sh); }
 
 // Warps per block: the requested query tile, or as many as fit 200 KB of
 // shared memory (at most 8); halved until the block fits.
@@ -713,22 +757,27 @@ uint32_t pick_wpb(const SearchShape &sh, size_t warp_bytes) {
 
 }  // namespace
 
+bool search_uses_compact(const SearchArgs &a, const SearchShape &sh) {
+    return sh.compact && a.compact_ok && a.prec == 0;
+}
+
 bool search_shape_valid(const SearchShape &sh) {
     const bool split_ok = sh.split == 0 || sh.split == 2 || sh.split == 4 || sh.split == 8;
     const bool wpb_ok = sh.warps_per_block == 0 || sh.warps_per_block == 1 || sh.warps_per_block == 2 ||
                         sh.warps_per_block == 4 || sh.warps_per_block == 8;
     const bool pf_ok = sh.prefetch == 0 || sh.prefetch == 2;
     const bool regs_ok = sh.regs == 0 || sh.regs == 64 || sh.regs == 80;
-    return split_ok && wpb_ok && pf_ok && regs_ok;
+    return split_ok && wpb_ok && pf_ok && regs_ok && sh.compact <= 1;
 }
 
 cudaError_t launch_search(SearchArgs &a, const SearchShape &sh, int num_sms, cudaStream_t st, uint32_t *grid_out) {
-    a.warp_smem_bytes = (uint32_t)search_warp_smem_bytes(a.D.ld, a.cap, a.rcap);
+    const bool cp = use_compact(a, sh);
+    a.warp_smem_bytes = (uint32_t)search_warp_smem_bytes(a.D.ld, a.cap, a.rcap, cp);
     const uint32_t wpb = pick_wpb(sh, a.warp_smem_bytes);
     if ((size_t)wpb * a.warp_smem_bytes > 227 * 1024) return cudaErrorInvalidValue;
     a.warps_per_block = wpb;
     size_t smem = (size_t)wpb * a.warp_smem_bytes;
-    SearchFn fn = search_fn(sh.split, sh.prefetch, a.prec, sh.regs);
+    SearchFn fn = search_fn(sh.split, sh.prefetch, a.prec, sh.regs, cp);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
@@ -746,10 +795,11 @@ cudaError_t launch_search(SearchArgs &a, const SearchShape &sh, int num_sms, cud
 }
 
 uint32_t search_max_slots(const SearchArgs &a, const SearchShape &sh, int num_sms) {
-    const size_t wb = search_warp_smem_bytes(a.D.ld, a.cap, a.rcap);
+    const bool cp = use_compact(a, sh);
+    const size_t wb = search_warp_smem_bytes(a.D.ld, a.cap, a.rcap, cp);
     const uint32_t wpb = pick_wpb(sh, wb);
     const size_t smem = (size_t)wpb * wb;
-    SearchFn fn = search_fn(sh.split, sh.prefetch, a.prec, sh.regs);
+    SearchFn fn = search_fn(sh.split, sh.prefetch, a.prec, sh.regs, cp);
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, wpb * 32, smem);

@@ -37,20 +37,27 @@ struct SearchArgs {
     const void *Xc;             // compressed rows (ld elements each)
     const float4 *cmeta;        // per row {error bound, scale, norm term, 0}
     uint32_t cap, rcap;         // smem capacities: max(K+P+1), max(K+1)
+    uint32_t compact_ok;        // the compact pool entry may be used: S >= 1 and every node's expansion
+                                //  (actual_M) <= (2^(31 - cp_idbits) - 1) S
+    uint32_t cp_idbits;         // compact pool: id bits of a pool word (ids < 2^cp_idbits)
     uint32_t warps_per_block, warp_smem_bytes;   // filled by launch_search
 };
 
 // Launch shape of the search kernel: the D-split (lanes per distance, 2/4/8;
 // 32/split candidates per pass), the query tile (warps = queries per block,
 // 1/2/4/8; 0 = as many as fit, at most 8), the L2 prefetch depth (0 or 2
-// neighbour batches) and the register budget per thread (64, or 80 for the
-// FP32 walk; 0 = 64).  Every shape computes the same bits.
+// neighbour batches), the register budget per thread (64, or 80 for the
+// FP32 walk; 0 = 64) and the pool entry (compact = 1: 8 bytes instead of 12,
+// FP32 walk only, where SearchArgs::compact_ok).  Every shape computes the
+// same bits.
 struct SearchShape {
-    uint32_t split = 4, warps_per_block = 0, prefetch = 2, regs = 64;
+    uint32_t split = 4, warps_per_block = 0, prefetch = 2, regs = 64, compact = 1;
 };
 bool search_shape_valid(const SearchShape &sh);
+// Whether a launch of shape sh with arguments a runs the compact pool entry.
+bool search_uses_compact(const SearchArgs &a, const SearchShape &sh);
 
-size_t search_warp_smem_bytes(uint32_t ld, uint32_t cap, uint32_t rcap);
+size_t search_warp_smem_bytes(uint32_t ld, uint32_t cap, uint32_t rcap, bool compact = false);
 // Upper bound of concurrently resident warps (= visited slots needed).
 uint32_t search_max_slots(const SearchArgs &a, const SearchShape &sh, int num_sms);
 cudaError_t launch_search(SearchArgs &a, const SearchShape &sh, int num_sms, cudaStream_t st, uint32_t *grid_out);

@@ -71,7 +71,8 @@ __device__ __forceinline__ uint32_t warp_update_knn(PD pd, PI pid, uint32_t *pm,
 
 // n successive UpdateKnnList calls (kgraph.cpp:503-512) by one warp in one
 // pass.  The candidates are the lanes set in `mask`, in lane order; each such
-// lane holds its candidate's distance di, id-with-flag idf and m|M word pmv.
+// lane holds its candidate's distance di, id-with-flag idf and m|M word pmv
+// (ignored when pm is null: a pool without m|M words).
 // They are inserted in order into the sorted pool pd/pid/pm of length L whose
 // capacity is cap (slot cap-1 is the overflow slot), L growing by one per
 // candidate up to cap-1.  Their ids are distinct and absent from the pool (the
@@ -122,15 +123,15 @@ __device__ __forceinline__ uint32_t warp_batch_insert(float *pd, uint32_t *pid, 
         const bool act = q >= (int)mina;
         float dv = 0.f;
         uint32_t iv = 0, mv = 0, sh = 0;
-        if (act) { dv = pd[q]; iv = pid[q]; mv = pm[q]; }
+        if (act) { dv = pd[q]; iv = pid[q]; if (pm) mv = pm[q]; }
         for (unsigned rest = mask; rest; rest &= rest - 1)
             sh += (__shfl_sync(FULL, ai, __ffs(rest) - 1) <= (uint32_t)q) ? 1u : 0u;
         __syncwarp();
-        if (act && (uint32_t)q + sh < Lf) { pd[q + sh] = dv; pid[q + sh] = iv; pm[q + sh] = mv; }
+        if (act && (uint32_t)q + sh < Lf) { pd[q + sh] = dv; pid[q + sh] = iv; if (pm) pm[q + sh] = mv; }
     }
     __syncwarp();
     const uint32_t fpos = ai + f;
-    if (me && fpos < Lf) { pd[fpos] = di; pid[fpos] = idf; pm[fpos] = pmv; }
+    if (me && fpos < Lf) { pd[fpos] = di; pid[fpos] = idf; if (pm) pm[fpos] = pmv; }
     __syncwarp();
     return Lf;
 }

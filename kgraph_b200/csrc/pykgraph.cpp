@@ -178,6 +178,7 @@ public:
         d["warps_per_block"] = t.warps_per_block;
         d["prefetch"] = t.prefetch;
         d["regs"] = t.regs;
+        d["compact"] = t.compact;
         d["ms"] = t.ms;
         d["default_ms"] = t.default_ms;
         return d;
