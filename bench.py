@@ -373,7 +373,8 @@ def run_workload(args, name):
     ctx = capi.Context(0)
     capi.set_verbosity(0)
     ctx.set_data(X, w["metric"])
-    ctx.set_join_precision(w["join"])
+    join_mode = args.join or w["join"]
+    ctx.set_join_precision(join_mode)
     ctx.build(**w["build"])            # first build of the process (one-time costs)
     cold_ms, _ = ctx.timing()
     info = ctx.build(**w["build"])
@@ -383,7 +384,7 @@ def run_workload(args, name):
            "dtype": "f32", "data": "synthetic", "config": {"workload": w["desc"], "N": n, "D": d, "queries": nq,
                                                            "build": w["build"], "metric": w["metric"]},
            "build": {"seconds": build_ms / 1000, "first_build_seconds": cold_ms / 1000, "info": info,
-                     "graph_launches": ctx.build_graph_launches(), "join": js}}
+                     "graph_launches": ctx.build_graph_launches(), "join_mode": join_mode, "join": js}}
     Xt = torch.as_tensor(X, dtype=torch.float64, device="cuda")
     Qt = torch.as_tensor(Q, dtype=torch.float64, device="cuda")
     gt_d, _ = exact_topk_fp64_chunked(Xt, Qt, 100 if w.get("mixed") else 10, torch)
@@ -550,6 +551,8 @@ def main():
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the reference's CPU build of the same graph (build parity, ~35 s on 16 threads)")
     ap.add_argument("--router-train", type=int, default=ROUTER_TRAIN)
+    ap.add_argument("--join", default=None, choices=["auto", "fp32", "bf16", "bf16_always", "fp8", "fp8_always"],
+                    help="local-join precision of a --workload run (default: the workload's own)")
     ap.add_argument("--workload", default="c2", choices=["c2"] + sorted(WORKLOADS),
                     help="c2 (default) is the headline 1M x 128 benchmark")
     args = ap.parse_args()
