@@ -272,6 +272,10 @@ typedef struct {
     unsigned entries;            /* entry nodes over all clusters */
     unsigned component_entries;  /* of which added for graph components no fine cluster reached */
     unsigned relabelled;         /* training labels changed by the refinement */
+    float label_s;               /* wall seconds: plain-search labels of the training queries */
+    float cluster_s;             /* normalisation, k-means, entry nodes, graph components */
+    float mlp_s;                 /* MLP epochs (all rounds) */
+    float refine_s;              /* refinement searches and regrouping */
 } kg_router_info;
 void kg_router_params_default(kg_router_params *p);
 /* Trains the router on the context's dataset and graph. */

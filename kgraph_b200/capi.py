@@ -51,7 +51,8 @@ class RouterParams(C.Structure):
 class RouterInfo(C.Structure):
     _fields_ = [("steps", C.c_uint), ("final_loss", C.c_float), ("train_accuracy", C.c_float),
                 ("empty_clusters", C.c_uint), ("entries", C.c_uint), ("component_entries", C.c_uint),
-                ("relabelled", C.c_uint)]
+                ("relabelled", C.c_uint), ("label_s", C.c_float), ("cluster_s", C.c_float), ("mlp_s", C.c_float),
+                ("refine_s", C.c_float)]
 
 
 class JoinStats(C.Structure):

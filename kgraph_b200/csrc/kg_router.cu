@@ -28,6 +28,7 @@
 //     query's own component.
 #include <cuda_bf16.h>
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <mutex>
 #include <numeric>
@@ -55,6 +56,30 @@ __global__ void features_kernel(const float *X, uint32_t ld, const uint32_t *row
         const uint32_t row = rows ? rows[r] : r;
         out[i] = __float2bfloat16_rn((X[(size_t)row * ld + c] - mean[c]) * inv_std[c]);
     }
+}
+
+// Per-dimension partial sums of a row block, in FP64 and a fixed order: block
+// b sums rows [b R, (b + 1) R) of x (pass 1) or of (x - mu)^2 (mu non-null),
+// into part[b * d + j].  The host adds the partials in block order, so the
+// result does not depend on scheduling.
+__global__ void colsum_kernel(const float *X, uint32_t ld, uint32_t n, uint32_t d, uint32_t R, const double *mu,
+                              double *part) {
+    const uint32_t r0 = blockIdx.x * R, r1 = min(n, r0 + R);
+    for (uint32_t j = threadIdx.x; j < d; j += blockDim.x) {
+        double s = 0.0;
+        const double m = mu ? mu[j] : 0.0;
+        for (uint32_t r = r0; r < r1; ++r) {
+            const double v = (double)X[(size_t)r * ld + j];
+            s += mu ? (v - m) * (v - m) : v;
+        }
+        part[(size_t)blockIdx.x * d + j] = s;
+    }
+}
+
+// Labels of a training batch: lab[i] = y[order[i]].
+__global__ void gather_labels_kernel(const int32_t *y, const uint32_t *order, uint32_t n, int32_t *lab) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) lab[i] = y[order[i]];
 }
 
 // Softmax cross-entropy, one warp per row: loss (summed into *loss), argmax
@@ -313,9 +338,10 @@ struct RouterState {
     DevBuf eoff, eids;                           // per cluster: its fine entry nodes (CSR)
     DevBuf w[3], b[3], wb[3], gw[3], gb[3], mw[3], vw[3], mb[3], vb[3];
     DevBuf X, H1, H1b, H2, H2b, Z, dZ, dZb, dH, dHb, lab, scal, topc;
+    DevBuf tq, tyo;                              // training: the queries (FP32 rows), their labels and order
     void release() {
         DevBuf *all[] = {&mean, &inv_std, &eoff, &eids, &X, &H1, &H1b, &H2, &H2b, &Z, &dZ, &dZb, &dH, &dHb, &lab,
-                         &scal, &topc};
+                         &scal, &topc, &tq, &tyo};
         for (DevBuf *p : all) p->release();
         for (int l = 0; l < 3; ++l) {
             DevBuf *ps[] = {&w[l], &b[l], &wb[l], &gw[l], &gb[l], &mw[l], &vw[l], &mb[l], &vb[l]};
@@ -581,6 +607,10 @@ extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const flo
             return set_error(ctx, KG_E_INVALID, "router sizes out of range (clusters 2..2048, entries 0..16, "
                                                 "probe 1..32)");
     }
+    using clk = std::chrono::steady_clock;
+    auto secs = [](clk::time_point a, clk::time_point b) { return (float)std::chrono::duration<double>(b - a).count(); };
+    const clk::time_point t_start = clk::now();
+    float refine_s = 0.f, mlp_s = 0.f;
     // 1. labels: the best node the plain search finds for each training query.
     //    The plain search starts every query of a call from the same P seeds
     //    (kgraph.cpp:444-453), so a region without a seed is missed by every
@@ -603,6 +633,7 @@ extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const flo
                                  topd.data() + a, cnt.data() + a, nullptr);
         if (rc != KG_OK) return rc;
     }
+    const clk::time_point t_labels = clk::now();
     std::unique_lock<std::mutex> lk(ctx->mu);   // released around the refinement's searches
     cudaSetDevice(ctx->device);
     cudaStream_t st = ctx->stream;
@@ -619,13 +650,30 @@ extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const flo
     DevBuf &s0 = ctx->build_scratch[20], &s1 = ctx->build_scratch[21], &s2 = ctx->build_scratch[22],
            &s3 = ctx->build_scratch[23];
 
-    // 2. normalisation over the dataset (per-dimension mean and 1/std)
-    std::vector<float> hX((size_t)N * D);
-    cudaMemcpy2D(hX.data(), D * 4, ctx->X.p, ctx->ld * 4, D * 4, N, cudaMemcpyDeviceToHost);
+    // 2. normalisation over the dataset (per-dimension mean and 1/std): FP64
+    //    partial sums per row block on the device, added on the host in order
     std::vector<double> mu(D, 0.0), var(D, 0.0);
-    for (size_t i = 0; i < (size_t)N * D; ++i) mu[i % D] += hX[i];
-    for (uint32_t j = 0; j < D; ++j) mu[j] /= N;
-    for (size_t i = 0; i < (size_t)N * D; ++i) { double t = hX[i] - mu[i % D]; var[i % D] += t * t; }
+    {
+        const uint32_t nb = std::max<uint32_t>(1u, std::min<uint32_t>(N, (uint32_t)ctx->num_sms * 8));
+        const uint32_t R = (N + nb - 1) / nb;
+        DevBuf part;
+        if ((e = part.reserve(((size_t)nb * D + D) * sizeof(double))) != cudaSuccess)
+            return cuda_fail(ctx, e, "router alloc");
+        double *dpart = part.as<double>(), *dmu = dpart + (size_t)nb * D;
+        std::vector<double> hpart((size_t)nb * D);
+        for (int pass = 0; pass < 2; ++pass) {
+            if (pass == 1) cudaMemcpyAsync(dmu, mu.data(), D * sizeof(double), cudaMemcpyHostToDevice, st);
+            colsum_kernel<<<nb, 128, 0, st>>>(ctx->X.as<float>(), ctx->ld, N, D, R, pass ? dmu : nullptr, dpart);
+            cudaMemcpyAsync(hpart.data(), dpart, hpart.size() * sizeof(double), cudaMemcpyDeviceToHost, st);
+            if ((e = cudaStreamSynchronize(st)) != cudaSuccess) { part.release(); return cuda_fail(ctx, e, "router stats"); }
+            std::vector<double> &acc = pass ? var : mu;
+            for (uint32_t b = 0; b < nb; ++b)
+                for (uint32_t j = 0; j < D; ++j) acc[j] += hpart[(size_t)b * D + j];
+            if (pass == 0)
+                for (uint32_t j = 0; j < D; ++j) mu[j] /= N;
+        }
+        part.release();
+    }
     std::vector<float> hm(D), hs(D);
     for (uint32_t j = 0; j < D; ++j) { hm[j] = (float)mu[j]; hs[j] = (float)(1.0 / std::sqrt(var[j] / N + 1e-6)); }
     if ((e = r.mean.reserve(D * 4)) != cudaSuccess || (e = r.inv_std.reserve(D * 4)) != cudaSuccess)
@@ -731,36 +779,44 @@ extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const flo
     }
     r.probe = std::max(1u, std::min(p->probe, C));
 
-    // 4. training set: query features and the cluster of each query's best node
+    const clk::time_point t_clusters = clk::now();
+    // 4. training set: the cluster of each query's best node.  The queries stay
+    //    on the device as FP32 rows; each step gathers and normalises its batch
+    //    there by the epoch's shuffled order, and nothing waits for the host
+    //    until an epoch run ends.
     std::vector<int32_t> ylab(ntrain);
     for (size_t i = 0; i < ntrain; ++i) ylab[i] = cnt[i] ? hlab[top[i] < N ? top[i] : 0] : 0;
-    std::vector<float> hq(ntrain * D);
-    cudaMemcpy2D(hq.data(), D * 4, train_queries, q_stride_bytes, D * 4, ntrain, cudaMemcpyDefault);
     init_weights(r, p->seed);
     const uint32_t B = p->batch;
-    DevBuf &tq = ctx->build_scratch[19];
+    DevBuf &tq = r.tq, &tyo = r.tyo;
+    if ((e = tq.reserve(ntrain * D * 4)) != cudaSuccess || (e = tyo.reserve(ntrain * 8)) != cudaSuccess)
+        return cuda_fail(ctx, e, "router alloc");
+    if ((e = cudaMemcpy2DAsync(tq.p, D * 4, train_queries, q_stride_bytes, D * 4, ntrain, cudaMemcpyDefault, st)) !=
+        cudaSuccess)
+        return cuda_fail(ctx, e, "router queries");
+    int32_t *dy = tyo.as<int32_t>();                                          // labels of the training queries
+    uint32_t *dorder = reinterpret_cast<uint32_t *>(dy + ntrain);             // the epoch's order
     std::vector<uint32_t> order(ntrain);
     for (size_t i = 0; i < ntrain; ++i) order[i] = (uint32_t)i;
     std::mt19937 rng(p->seed + 1);
-    std::vector<float> hbatch((size_t)std::max<uint32_t>(B, 1) * D);
-    std::vector<int32_t> hy(std::max<uint32_t>(B, 1));
     float last_loss = 0.f;
     unsigned step = 0;
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
     const size_t full = ntrain < B ? ntrain : ntrain / B * B;   // the last partial batch is dropped
     auto run_epochs = [&](uint32_t epochs) -> int {
+    const clk::time_point t0 = clk::now();
+    // pageable sources: each copy has read its host buffer when it returns
+    cudaMemcpyAsync(dy, ylab.data(), ntrain * 4, cudaMemcpyHostToDevice, st);
+    uint32_t last_bs = 0;
     for (uint32_t ep = 0; ep < epochs; ++ep) {
         std::shuffle(order.begin(), order.end(), rng);
+        cudaMemcpyAsync(dorder, order.data(), ntrain * 4, cudaMemcpyHostToDevice, st);
         for (size_t s0i = 0; s0i < full; s0i += B) {
             const uint32_t bs = (uint32_t)std::min<size_t>(B, full - s0i);
-            for (uint32_t i = 0; i < bs; ++i) {
-                const size_t qi = order[s0i + i];
-                std::copy(hq.begin() + qi * D, hq.begin() + (qi + 1) * D, hbatch.begin() + (size_t)i * D);
-                hy[i] = ylab[qi];
-            }
-            int rc = stage_queries(ctx, r, hbatch.data(), bs, D * 4, tq);
-            if (rc != KG_OK) return rc;
-            cudaMemcpyAsync(r.lab.p, hy.data(), bs * 4, cudaMemcpyHostToDevice, st);
+            features_kernel<<<blocks_for((size_t)bs * D), 256, 0, st>>>(tq.as<float>(), D, dorder + s0i, bs, D,
+                                                                        r.mean.as<float>(), r.inv_std.as<float>(),
+                                                                        r.X.as<__nv_bfloat16>());
+            gather_labels_kernel<<<(bs + 255) / 256, 256, 0, st>>>(dy, dorder + s0i, bs, r.lab.as<int32_t>());
             cudaMemsetAsync(r.scal.p, 0, 8, st);
             forward(st, r, bs);
             backward(st, r, bs);
@@ -776,12 +832,14 @@ extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const flo
                                                                  r.mb[l].as<float>(), r.vb[l].as<float>(), nullptr,
                                                                  out[l], p->lr, b1, b2, c1, c2, eps);
             }
-            float hl = 0.f;
-            cudaMemcpyAsync(&hl, r.scal.p, 4, cudaMemcpyDeviceToHost, st);
-            if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "router train");
-            last_loss = hl / bs;
+            last_bs = bs;
         }
     }
+    float hl = 0.f;   // the last step's summed loss
+    cudaMemcpyAsync(&hl, r.scal.p, 4, cudaMemcpyDeviceToHost, st);
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "router train");
+    if (last_bs) last_loss = hl / last_bs;
+    mlp_s += secs(t0, clk::now());
     return KG_OK;
     };
     int rc0 = run_epochs(p->epochs);
@@ -793,6 +851,7 @@ extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const flo
     std::vector<float> sd;
     unsigned relabelled = 0;
     for (uint32_t round = 0; round < p->refine; ++round) {
+        const clk::time_point tr = clk::now();
         r.trained = true;
         const unsigned m = 3, ld = m + 1;   // the reference requires init < K
         sids.assign(ntrain * ld, 0u);
@@ -860,6 +919,7 @@ extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const flo
             if ((rc = install_entries()) != KG_OK) return rc;
             for (size_t i = 0; i < ntrain; ++i) ylab[i] = cnt[i] ? hlab[top[i] < N ? top[i] : 0] : 0;
         }
+        refine_s += secs(tr, clk::now());
         if ((rc = run_epochs(p->epochs)) != KG_OK) return rc;
     }
     // accuracy of the final weights on the first min(ntrain, 4096) training rows
@@ -867,11 +927,13 @@ extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const flo
     {
         const size_t n = std::min<size_t>(ntrain, 4096);
         unsigned hits_total = 0;
+        cudaMemcpyAsync(dy, ylab.data(), n * 4, cudaMemcpyHostToDevice, st);
         for (size_t c0 = 0; c0 < n; c0 += r.batch) {
             const uint32_t bs = (uint32_t)std::min<size_t>(r.batch, n - c0);
-            int rc = stage_queries(ctx, r, hq.data() + c0 * D, bs, D * 4, tq);
-            if (rc != KG_OK) return rc;
-            cudaMemcpyAsync(r.lab.p, ylab.data() + c0, bs * 4, cudaMemcpyHostToDevice, st);
+            features_kernel<<<blocks_for((size_t)bs * D), 256, 0, st>>>(tq.as<float>() + c0 * D, D, nullptr, bs, D,
+                                                                        r.mean.as<float>(), r.inv_std.as<float>(),
+                                                                        r.X.as<__nv_bfloat16>());
+            cudaMemcpyAsync(r.lab.p, dy + c0, bs * 4, cudaMemcpyDeviceToDevice, st);
             cudaMemsetAsync(r.scal.p, 0, 8, st);
             forward(st, r, bs);
             softmax_ce_kernel<<<(bs * 32 + 255) / 256, 256, 0, st>>>(r.Z.as<float>(), r.lab.as<int32_t>(), bs, r.C,
@@ -886,6 +948,8 @@ extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const flo
     }
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "router train");
     r.trained = true;
+    tq.release();    // the training set is not needed for seeding
+    tyo.release();
     if (info) {
         info->steps = step;
         info->final_loss = last_loss;
@@ -894,6 +958,10 @@ extern "C" int kg_router_train(kg_ctx *ctx, const kg_router_params *p, const flo
         info->entries = r.entries_total;
         info->component_entries = r.component_entries;
         info->relabelled = relabelled;
+        info->label_s = secs(t_start, t_labels);
+        info->cluster_s = secs(t_labels, t_clusters);
+        info->mlp_s = mlp_s;
+        info->refine_s = refine_s;
     }
     return check_device_error(ctx, "router");
 }
