@@ -30,10 +30,12 @@ extern "C" int kg_tc_gemm_check(kg_ctx *ctx, int M, int N, int K, const uint16_t
     if (M <= 0 || N <= 0 || K < 0 || !A || !B || !C || lda <= 0 || ldb <= 0 || ldc < N)
         return set_error(ctx, KG_E_INVALID, "bad GEMM shape");
     const size_t a_el = (size_t)(ta ? K : M) * lda, b_el = (size_t)(tb ? N : K) * ldb, c_el = (size_t)M * ldc;
-    Tmp dA, dB, dC, dbias;
+    Tmp dA, dB, dC, dbias, dws;
+    const size_t wsb = tc_gemm_workspace_bytes(M, N, K);
     cudaError_t e;
     if ((e = dA.alloc(a_el * 2)) != cudaSuccess || (e = dB.alloc(b_el * 2)) != cudaSuccess ||
-        (e = dC.alloc(c_el * 4)) != cudaSuccess || (bias && (e = dbias.alloc((size_t)N * 4)) != cudaSuccess))
+        (e = dC.alloc(c_el * 4)) != cudaSuccess || (bias && (e = dbias.alloc((size_t)N * 4)) != cudaSuccess) ||
+        (wsb && (e = dws.alloc(wsb)) != cudaSuccess))
         return cuda_fail(ctx, e, "alloc");
     cudaStream_t st = ctx->stream;
     cudaMemcpyAsync(dA.p, A, a_el * 2, cudaMemcpyDefault, st);
@@ -42,7 +44,7 @@ extern "C" int kg_tc_gemm_check(kg_ctx *ctx, int M, int N, int K, const uint16_t
     if (bias) cudaMemcpyAsync(dbias.p, bias, (size_t)N * 4, cudaMemcpyDefault, st);
     tc_gemm(st, M, N, K, static_cast<const __nv_bfloat16 *>(dA.p), lda, ta, static_cast<const __nv_bfloat16 *>(dB.p),
             ldb, tb, static_cast<float *>(dC.p), ldc, nullptr, bias ? static_cast<const float *>(dbias.p) : nullptr,
-            relu, beta, ctx->errw.as<uint32_t>());
+            relu, beta, static_cast<float *>(dws.p), wsb, ctx->errw.as<uint32_t>());
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "tc_gemm launch");
     cudaMemcpyAsync(C, dC.p, c_el * 4, cudaMemcpyDefault, st);
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "tc_gemm");

@@ -316,11 +316,13 @@ __global__ void __launch_bounds__(RANK_WARPS * 32) seed_rank_kernel(DataView D, 
     }
 }
 
-// Every product of the router runs on the tensor cores (kg_gemm.cu).
-void gemm(cudaStream_t st, uint32_t *err, int M, int N, int K, const __nv_bfloat16 *A, int lda, int ta,
-          const __nv_bfloat16 *B, int ldb, int tb, float *C, int ldc, __nv_bfloat16 *Cb, const float *bias, int relu,
-          float beta = 0.f) {
-    tc_gemm(st, M, N, K, A, lda, ta, B, ldb, tb, C, ldc, Cb, bias, relu, beta, err);
+// Every product of the router runs on the tensor cores (kg_gemm.cu); ws (may
+// be null) is the scratch of the K-split products.
+void gemm(cudaStream_t st, uint32_t *err, const DevBuf *ws, int M, int N, int K, const __nv_bfloat16 *A, int lda,
+          int ta, const __nv_bfloat16 *B, int ldb, int tb, float *C, int ldc, __nv_bfloat16 *Cb, const float *bias,
+          int relu, float beta = 0.f) {
+    tc_gemm(st, M, N, K, A, lda, ta, B, ldb, tb, C, ldc, Cb, bias, relu, beta, ws ? ws->as<float>() : nullptr,
+            ws ? ws->bytes : 0, err);
 }
 
 int blocks_for(size_t n, int per = 256) { return (int)std::min<size_t>((n + per - 1) / per, 148 * 32); }
@@ -338,10 +340,11 @@ struct RouterState {
     DevBuf eoff, eids;                           // per cluster: its fine entry nodes (CSR)
     DevBuf w[3], b[3], wb[3], gw[3], gb[3], mw[3], vw[3], mb[3], vb[3];
     DevBuf X, H1, H1b, H2, H2b, Z, dZ, dZb, dH, dHb, lab, scal, topc;
+    DevBuf gws;                                  // K-split scratch of the backward products
     DevBuf tq, tyo;                              // training: the queries (FP32 rows), their labels and order
     void release() {
         DevBuf *all[] = {&mean, &inv_std, &eoff, &eids, &X, &H1, &H1b, &H2, &H2b, &Z, &dZ, &dZb, &dH, &dHb, &lab,
-                         &scal, &topc, &tq, &tyo};
+                         &scal, &topc, &tq, &tyo, &gws};
         for (DevBuf *p : all) p->release();
         for (int l = 0; l < 3; ++l) {
             DevBuf *ps[] = {&w[l], &b[l], &wb[l], &gw[l], &gb[l], &mw[l], &vw[l], &mb[l], &vb[l]};
@@ -377,17 +380,24 @@ cudaError_t alloc_router(RouterState &r, uint32_t batch) {
         (e = r.dH.reserve(B * r.H * 4)) != cudaSuccess || (e = r.dHb.reserve(B * r.H * 2)) != cudaSuccess ||
         (e = r.lab.reserve(B * 4)) != cudaSuccess || (e = r.scal.reserve(64)) != cudaSuccess)
         return e;
+    // the backward products' K splits (the forward ones are not split at these shapes)
+    const int Bi = (int)batch, D = (int)r.D, H = (int)r.H, C = (int)r.C;
+    const size_t wsb = std::max({tc_gemm_workspace_bytes(H, C, Bi), tc_gemm_workspace_bytes(Bi, H, C),
+                                 tc_gemm_workspace_bytes(H, H, Bi), tc_gemm_workspace_bytes(Bi, H, H),
+                                 tc_gemm_workspace_bytes(D, H, Bi), tc_gemm_workspace_bytes(Bi, H, D),
+                                 tc_gemm_workspace_bytes(Bi, C, H)});
+    if (wsb && (e = r.gws.reserve(wsb)) != cudaSuccess) return e;
     r.batch = batch;
     return cudaSuccess;
 }
 
 // Forward of B rows already in r.X (BF16 features): H1, H2, Z.
 void forward(cudaStream_t st, RouterState &r, int B) {
-    gemm(st, r.err, B, r.H, r.D, r.X.as<__nv_bfloat16>(), r.D, 0, r.wb[0].as<__nv_bfloat16>(), r.H, 0, r.H1.as<float>(), r.H,
+    gemm(st, r.err, &r.gws, B, r.H, r.D, r.X.as<__nv_bfloat16>(), r.D, 0, r.wb[0].as<__nv_bfloat16>(), r.H, 0, r.H1.as<float>(), r.H,
          r.H1b.as<__nv_bfloat16>(), r.b[0].as<float>(), 1);
-    gemm(st, r.err, B, r.H, r.H, r.H1b.as<__nv_bfloat16>(), r.H, 0, r.wb[1].as<__nv_bfloat16>(), r.H, 0, r.H2.as<float>(), r.H,
+    gemm(st, r.err, &r.gws, B, r.H, r.H, r.H1b.as<__nv_bfloat16>(), r.H, 0, r.wb[1].as<__nv_bfloat16>(), r.H, 0, r.H2.as<float>(), r.H,
          r.H2b.as<__nv_bfloat16>(), r.b[1].as<float>(), 1);
-    gemm(st, r.err, B, r.C, r.H, r.H2b.as<__nv_bfloat16>(), r.H, 0, r.wb[2].as<__nv_bfloat16>(), r.C, 0, r.Z.as<float>(), r.C,
+    gemm(st, r.err, &r.gws, B, r.C, r.H, r.H2b.as<__nv_bfloat16>(), r.H, 0, r.wb[2].as<__nv_bfloat16>(), r.C, 0, r.Z.as<float>(), r.C,
          nullptr, r.b[2].as<float>(), 0);
 }
 
@@ -398,24 +408,24 @@ void backward(cudaStream_t st, RouterState &r, int B) {
     softmax_ce_kernel<<<(B * 32 + 255) / 256, 256, 0, st>>>(r.Z.as<float>(), r.lab.as<int32_t>(), B, r.C,
                                                             r.dZ.as<float>(), r.dZb.as<__nv_bfloat16>(), loss, hits);
     // layer 3: dW3 = H2^T dZ, db3, dH2 = dZ W3^T
-    gemm(st, r.err, r.H, r.C, B, r.H2b.as<__nv_bfloat16>(), r.H, 1, r.dZb.as<__nv_bfloat16>(), r.C, 0, r.gw[2].as<float>(), r.C,
+    gemm(st, r.err, &r.gws, r.H, r.C, B, r.H2b.as<__nv_bfloat16>(), r.H, 1, r.dZb.as<__nv_bfloat16>(), r.C, 0, r.gw[2].as<float>(), r.C,
          nullptr, nullptr, 0);
     colsum_kernel<<<(r.C + 255) / 256, 256, 0, st>>>(r.dZ.as<float>(), B, r.C, r.gb[2].as<float>());
-    gemm(st, r.err, B, r.H, r.C, r.dZb.as<__nv_bfloat16>(), r.C, 0, r.wb[2].as<__nv_bfloat16>(), r.C, 1, r.dH.as<float>(), r.H,
+    gemm(st, r.err, &r.gws, B, r.H, r.C, r.dZb.as<__nv_bfloat16>(), r.C, 0, r.wb[2].as<__nv_bfloat16>(), r.C, 1, r.dH.as<float>(), r.H,
          nullptr, nullptr, 0);
     relu_grad_kernel<<<blocks_for((size_t)B * r.H), 256, 0, st>>>(r.dH.as<float>(), r.H2.as<float>(),
                                                                   r.dHb.as<__nv_bfloat16>(), (size_t)B * r.H);
     // layer 2
-    gemm(st, r.err, r.H, r.H, B, r.H1b.as<__nv_bfloat16>(), r.H, 1, r.dHb.as<__nv_bfloat16>(), r.H, 0, r.gw[1].as<float>(), r.H,
+    gemm(st, r.err, &r.gws, r.H, r.H, B, r.H1b.as<__nv_bfloat16>(), r.H, 1, r.dHb.as<__nv_bfloat16>(), r.H, 0, r.gw[1].as<float>(), r.H,
          nullptr, nullptr, 0);
     colsum_kernel<<<(r.H + 255) / 256, 256, 0, st>>>(r.dH.as<float>(), B, r.H, r.gb[1].as<float>());
     // dH1 = dH2 W2^T (into r.dZ as scratch: B x H fits), then the ReLU mask
-    gemm(st, r.err, B, r.H, r.H, r.dHb.as<__nv_bfloat16>(), r.H, 0, r.wb[1].as<__nv_bfloat16>(), r.H, 1, r.dZ.as<float>(), r.H,
+    gemm(st, r.err, &r.gws, B, r.H, r.H, r.dHb.as<__nv_bfloat16>(), r.H, 0, r.wb[1].as<__nv_bfloat16>(), r.H, 1, r.dZ.as<float>(), r.H,
          nullptr, nullptr, 0);
     relu_grad_kernel<<<blocks_for((size_t)B * r.H), 256, 0, st>>>(r.dZ.as<float>(), r.H1.as<float>(),
                                                                   r.dHb.as<__nv_bfloat16>(), (size_t)B * r.H);
     // layer 1
-    gemm(st, r.err, r.D, r.H, B, r.X.as<__nv_bfloat16>(), r.D, 1, r.dHb.as<__nv_bfloat16>(), r.H, 0, r.gw[0].as<float>(), r.H,
+    gemm(st, r.err, &r.gws, r.D, r.H, B, r.X.as<__nv_bfloat16>(), r.D, 1, r.dHb.as<__nv_bfloat16>(), r.H, 0, r.gw[0].as<float>(), r.H,
          nullptr, nullptr, 0);
     colsum_kernel<<<(r.H + 255) / 256, 256, 0, st>>>(r.dZ.as<float>(), B, r.H, r.gb[0].as<float>());
 }
@@ -485,7 +495,7 @@ cudaError_t kmeans_run(cudaStream_t st, uint32_t *err, const __nv_bfloat16 *F, u
         if (!tc_assign(st, (int)n, (int)D, F, centb, (int)C, cn, lab, best, err)) {
             for (uint32_t r0 = 0; r0 < n; r0 += brows) {
                 const uint32_t rows = std::min<uint32_t>(brows, n - r0);
-                gemm(st, err, rows, C, D, F + (size_t)r0 * D, D, 0, centb, D, 1, block.as<float>(), C, nullptr, nullptr,
+                gemm(st, err, nullptr, rows, C, D, F + (size_t)r0 * D, D, 0, centb, D, 1, block.as<float>(), C, nullptr, nullptr,
                      0);
                 argmin_kernel<<<(rows * 32 + 255) / 256, 256, 0, st>>>(block.as<float>(), cn, rows, C, lab + r0,
                                                                        best + r0);

@@ -1,18 +1,31 @@
 // Fifth-generation tensor core (tcgen05) building blocks for sm_100a: TMEM
 // allocation, shared-memory operand descriptors, the BF16 MMA with an FP32
-// accumulator in TMEM, its completion barrier and the TMEM read-back.
+// accumulator in TMEM, its completion barrier, the TMEM read-back, and the
+// tensor-memory-accelerator (TMA) tile loads that feed it.
 //
-// Operands are staged by the threads themselves (no TMA) in the K-major,
-// no-swizzle "core matrix" layout the UMMA descriptor describes: 8 rows x
-// 16 bytes per core matrix; row r, element k of a tile with K columns sits at
-// byte (r/8)*SBO + (k/8)*LBO + (r%8)*16 + (k%8)*2 with LBO = 128 (the next 8
-// elements along K) and SBO = K*16 (the next 8 rows).  One MMA consumes K = 16
-// (two core matrices along K); the next K step starts 256 bytes further.
+// Two operand layouts are described.
+//
+// (1) No swizzle, K-major "core matrices", staged by the threads themselves:
+// 8 rows x 16 bytes per core matrix; row r, element k of a tile with K columns
+// sits at byte (r/8)*SBO + (k/8)*LBO + (r%8)*16 + (k%8)*2 with LBO = 128 (the
+// next 8 elements along K) and SBO = K*16 (the next 8 rows).  One MMA consumes
+// K = 16 (two core matrices along K); the next K step starts 256 bytes further.
+//
+// (2) 128-byte swizzle, written by TMA (cp.async.bulk.tensor, tensor map with
+// CU_TENSOR_MAP_SWIZZLE_128B, box inner extent 64 BF16 = 128 bytes).  A
+// K-major tile is rows x 128 bytes (64 elements of K per row), 8-row groups
+// 1024 bytes apart (SBO = 1024; LBO unused); a K = 16 step advances the start
+// address by 32 bytes inside the swizzle atom.  An MN-major tile (the operand
+// stored K x MN, MN contiguous) is one 64 (MN) x 64 (K) box per 64 columns of
+// MN: 64 rows of K x 128 bytes, 8-row groups 1024 bytes apart (SBO), the
+// next 64 columns of MN one box (8192 bytes) further (LBO); a K = 16 step
+// advances the start address by 2048 bytes.  Tiles start on 1024-byte
+// boundaries so the swizzle phase is that of the address.
 //
 // Descriptor bit layouts follow the sm_100 UMMA descriptors (SmemDescriptor:
-// start>>4 @0, LBO>>4 @16, SBO>>4 @32, version 1 @46, layout type @61;
-// InstrDescriptor: D format @4, A/B format @7/@10, A/B major @15/@16,
-// N>>3 @17, M>>4 @24).
+// start>>4 @0, LBO>>4 @16, SBO>>4 @32, version 1 @46, layout type @61 (0 no
+// swizzle, 2 128-byte swizzle); InstrDescriptor: D format @4, A/B format
+// @7/@10, A/B major @15/@16 (1 = MN-major), N>>3 @17, M>>4 @24).
 #pragma once
 #include <cstdint>
 #include <cuda_bf16.h>
@@ -36,9 +49,18 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
     return d;
 }
 
+// The same with the 128-byte swizzle layout type.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return smem_desc(saddr, lbo, sbo) | ((uint64_t)2 << 61);
+}
+
 // kind::f16 instruction descriptor: BF16 x BF16 -> FP32, both operands K-major.
 __host__ __device__ constexpr uint32_t idesc_bf16_f32(uint32_t M, uint32_t N) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
+}
+// The same with A and / or B MN-major (stored K x M / K x N, MN contiguous).
+__host__ __device__ constexpr uint32_t idesc_bf16_f32_major(uint32_t M, uint32_t N, uint32_t a_mn, uint32_t b_mn) {
+    return idesc_bf16_f32(M, N) | (a_mn << 15) | (b_mn << 16);
 }
 
 // kind::f8f6f4 instruction descriptor: E4M3 x E4M3 (format code 0 for both)
@@ -72,6 +94,27 @@ __device__ __forceinline__ void tmem_free(uint32_t taddr, uint32_t cols) {
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// One thread: arm *bar for `bytes` of TMA transactions (and arrive once).
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+// One thread: a plain arrive on *bar.
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// One thread: TMA load of the box at (x, y) of a 2-D tensor map (a kernel
+// parameter declared __grid_constant__) into shared memory at dst; completion
+// is counted in bytes on *bar.  This GPU's memory only, no multicast; x times
+// the element size is a multiple of 16 bytes at every call site.
+__device__ __forceinline__ void tma_load_2d(void *dst, const void *tmap, int x, int y, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+            "r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(smem_addr(bar))
+        : "memory");
 }
 
 // One thread: D[tmem] (+)= A[smem] * B[smem]^T for one K=16 step.

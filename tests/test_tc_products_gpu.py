@@ -5,8 +5,9 @@ k-means assignment (tc_assign_kernel), called through their C-ABI check entry
 points and compared with an FP64 evaluation of the same BF16 operands.  The
 shapes are the MLP's (4096-row batches, 128 -> 256 -> 256 -> 1024) forward
 and backward products, K that is not a multiple of the 64-wide K chunk, M and N
-that are not multiples of the 128-wide tile, and the assignment of 10k rows to
-8,192 centroids at D = 128 and D = 96.
+that are not multiples of the 128-wide tile, products split along K, both the
+TMA-fed path (16-byte aligned row pitches) and the register-staged fallback,
+and the assignment of 10k rows to 8,192 centroids at D = 128 and D = 96.
 
 Tolerance: products of BF16 values are exact in FP32; the K-long FP32
 accumulation is bounded by K * 2^-22 * sum_k |a_k b_k| (twice the unit
@@ -70,6 +71,15 @@ def _check_gemm(ctx, M, N, K, ta, tb, seed, bias=False, relu=False, beta=0.0):
     (256, 1024, 4096, True, False, {}),                              # dW3 = H^T dY
     (4096, 256, 1024, False, True, {}),                              # dH = dY W3^T
     (128, 256, 4096, True, False, {}),                               # dW1 = X^T dH1
+    (256, 256, 4096, True, False, {}),                               # dW2 = H1^T dH2 (split along K)
+    (4096, 256, 256, False, True, {}),                               # dH1 = dH2 W2^T
+    # TMA path (16-byte aligned pitches) at ragged shapes: partial tiles, K not a multiple of 64, splits
+    (1000, 200, 104, False, False, dict(beta=0.5, bias=True)),
+    (136, 264, 72, True, True, dict(relu=True)),
+    (200, 136, 4000, True, True, dict(bias=True)),
+    (72, 1000, 3000, True, False, dict(beta=-1.0)),
+    (300, 40, 8, False, True, {}),
+    # register-staged fallback (pitches that TMA cannot address)
     (1000, 200, 100, False, False, dict(beta=0.5, bias=True)),       # ragged M, N; K not a multiple of 64
     (130, 257, 65, True, True, dict(relu=True)),                     # ragged, both transposed
     (1, 1, 1, False, False, {}),
@@ -78,7 +88,8 @@ def test_tc_gemm_matches_fp64(gpu_ctx, M, N, K, ta, tb, extra):
     _check_gemm(gpu_ctx, M, N, K, ta, tb, seed=M * 7 + N * 3 + K, **extra)
 
 
-@pytest.mark.parametrize("n,C,D", [(10_000, 8192, 128), (10_000, 8192, 96), (3000, 1000, 100), (129, 1, 16)])
+@pytest.mark.parametrize("n,C,D", [(10_000, 8192, 128), (10_000, 8192, 96), (3000, 1000, 100), (129, 1, 16),
+                                   (5000, 300, 64), (1000, 129, 256), (777, 4100, 40)])
 def test_tc_assign_matches_fp64_argmin(gpu_ctx, n, C, D):
     rng = np.random.default_rng(n + C + D)
     cent_f = rng.standard_normal((C, D)).astype(np.float32)
