@@ -117,14 +117,20 @@ __device__ __forceinline__ uint32_t warp_batch_insert(float *pd, uint32_t *pid, 
     *min_rank = mr;
     const uint32_t Lf = min(L + n, cap - 1);
     // move pool entries q >= mina up by #{j : a_j <= q}, top-down (each chunk's
-    // loads precede the next chunk's stores, which reach at most this chunk)
+    // loads precede the next chunk's stores, which reach at most this chunk).
+    // For the chunk [top - 31, top]: the candidates with a_j <= top - 31 count
+    // for every lane (one ballot); only those with a_j inside the chunk are
+    // compared lane by lane.
     for (int top = (int)L - 1; top >= (int)mina; top -= 32) {
         const int q = top - lane;
         const bool act = q >= (int)mina;
         float dv = 0.f;
-        uint32_t iv = 0, mv = 0, sh = 0;
+        uint32_t iv = 0, mv = 0;
         if (act) { dv = pd[q]; iv = pid[q]; if (pm) mv = pm[q]; }
-        for (unsigned rest = mask; rest; rest &= rest - 1)
+        const int bot = top - 31;
+        const unsigned below = __ballot_sync(FULL, me && (int)ai <= bot);
+        uint32_t sh = __popc(below);
+        for (unsigned rest = __ballot_sync(FULL, me && (int)ai > bot && (int)ai <= top); rest; rest &= rest - 1)
             sh += (__shfl_sync(FULL, ai, __ffs(rest) - 1) <= (uint32_t)q) ? 1u : 0u;
         __syncwarp();
         if (act && (uint32_t)q + sh < Lf) { pd[q + sh] = dv; pid[q + sh] = iv; if (pm) pm[q + sh] = mv; }
