@@ -340,6 +340,34 @@ int kg_tc_assign_check(kg_ctx *ctx, const uint16_t *F, int n, int D, const uint1
 enum { KG_JOIN_AUTO = 0, KG_JOIN_FP32 = 1, KG_JOIN_BF16 = 2, KG_JOIN_BF16_ALWAYS = 3, KG_JOIN_FP8 = 4,
        KG_JOIN_FP8_ALWAYS = 5 };
 int kg_set_join_precision(kg_ctx *ctx, int mode);
+
+/* How the FP32 local join applies its inserts (Nhood::parallel_try_insert,
+ * kgraph.cpp:723-736).  No counterpart in the reference, whose threads insert
+ * under a per-node lock as they go.
+ *   KG_INSERTS_LOCKED    the same: one warp takes the target's lock per offer;
+ *   KG_INSERTS_DEFERRED  the join records every offer that passes the unlocked
+ *                        radius test; the offers are then grouped by target and
+ *                        each pool takes its own in one merge, in ascending
+ *                        (distance, id) order -- a serial order of the same
+ *                        inserts that the reference's threads can produce, with
+ *                        the same duplicate, radius, L and `found` rules; offers
+ *                        beyond the record buffer's capacity (sized from free
+ *                        device memory, at most 20 GB) are inserted under the
+ *                        lock during the join;
+ *   KG_INSERTS_AUTO      (default) KG_INSERTS_DEFERRED.
+ * The tensor-core joins (KG_JOIN_BF16 / KG_JOIN_FP8 iterations) always lock. */
+enum { KG_INSERTS_AUTO = 0, KG_INSERTS_LOCKED = 1, KG_INSERTS_DEFERRED = 2 };
+int kg_set_join_inserts(kg_ctx *ctx, int mode);
+/* Check entry point of the deferred inserts' merge, on caller data: n pools of
+ * L+1 entries (rows of L+1: distances, ids with the new-flag in bit 31), their
+ * list lengths and radii (updated in place), and n_off offers (target pool,
+ * candidate id, distance, source node with bit 31 set for a pair's x <- y
+ * offer); found[source] is set to 1 where such an offer lands below K (other
+ * entries 0).  A pool's offers are merged in ascending (distance, id) order in
+ * passes of at most 512.  No counterpart in the reference. */
+int kg_join_merge_check(kg_ctx *ctx, unsigned n, unsigned L, unsigned K, float *pool_d, uint32_t *pool_i,
+                        uint32_t *nodeL, float *radius, size_t n_off, const uint32_t *target, const uint32_t *cand,
+                        const float *dist, const uint32_t *src, uint32_t *found);
 /* Counters of the last kg_build's join.  mode: KG_JOIN_BF16 or KG_JOIN_FP8 when
  * any iteration ran the tensor-core filter (tc_iterations of them).  pairs: join
  * pairs (IndexInfo.cost * N(N-1)/2 summed over iterations); rechecked: pairs

@@ -21,7 +21,7 @@ SYMBOLS = [
     "kg_graph_export", "kg_graph_import", "kg_search_batch", "kg_reverse", "kg_prune", "kg_last_timing",
     "kg_last_search_work", "kg_search_batch_noalloc", "kg_noalloc_scratch_bytes",
     "kg_router_params_default", "kg_router_train", "kg_router_seeds", "kg_router_gradients", "kg_last_router_timing",
-    "kg_set_join_precision", "kg_last_join_stats", "kg_last_build_graphs", "kg_search_autotune",
+    "kg_set_join_precision", "kg_set_join_inserts", "kg_join_merge_check", "kg_last_join_stats", "kg_last_build_graphs", "kg_search_autotune",
     "kg_set_search_tuning", "kg_get_search_tuning", "kg_last_search_shape", "kg_set_search_precision",
     "kg_last_search_filter",
     "kg_filter_bounds", "kg_router_search", "kg_tc_gemm_check", "kg_tc_assign_check", "kg_last_build_work",
@@ -86,6 +86,7 @@ class BruteforceStats(C.Structure):
 
 
 BRUTEFORCE = {"auto": 0, "scan": 1, "tensor": 2}
+INSERTS = {"auto": 0, "locked": 1, "deferred": 2}
 
 
 class SearchParams(C.Structure):
@@ -129,6 +130,8 @@ def lib():
         L.kg_router_gradients.argtypes = [vp, C.c_uint, C.c_uint, C.c_uint, vp, vp, vp, C.c_uint,
                                           C.POINTER(C.c_float), vp]
         L.kg_set_join_precision.argtypes = [vp, C.c_int]
+        L.kg_set_join_inserts.argtypes = [vp, C.c_int]
+        L.kg_join_merge_check.argtypes = [vp, C.c_uint, C.c_uint, C.c_uint, vp, vp, vp, vp, sz, vp, vp, vp, vp, vp]
         L.kg_last_join_stats.argtypes = [vp, C.POINTER(JoinStats)]
         L.kg_last_build_graphs.argtypes = [vp, C.POINTER(C.c_uint)]
         L.kg_search_autotune.argtypes = [vp, vp, sz, sz, C.POINTER(SearchParams), vp, vp, vp, sz,
@@ -383,6 +386,27 @@ class Context:
     def set_join_precision(self, mode):
         """'auto' (BF16 tensor-core join for d >= 64), 'fp32', 'bf16' or 'bf16_always'."""
         self._check(self.L.kg_set_join_precision(self.h, JOIN[mode] if isinstance(mode, str) else int(mode)))
+
+    def join_merge_check(self, L, K, pool_d, pool_i, nodeL, radius, target, cand, dist, src):
+        """kg_join_merge_check: the deferred-insert merge on caller pools (n x (L+1)) and offers.
+        Returns (pool_d, pool_i, nodeL, radius, found)."""
+        pd = np.ascontiguousarray(pool_d, np.float32).copy()
+        pi = np.ascontiguousarray(pool_i, np.uint32).copy()
+        nl = np.ascontiguousarray(nodeL, np.uint32).copy()
+        rd = np.ascontiguousarray(radius, np.float32).copy()
+        n = pd.shape[0]
+        t = np.ascontiguousarray(target, np.uint32)
+        c = np.ascontiguousarray(cand, np.uint32)
+        d = np.ascontiguousarray(dist, np.float32)
+        s_ = np.ascontiguousarray(src, np.uint32)
+        found = np.zeros(n, np.uint32)
+        self._check(self.L.kg_join_merge_check(self.h, n, L, K, _ptr(pd), _ptr(pi), _ptr(nl), _ptr(rd), len(t),
+                                               _ptr(t), _ptr(c), _ptr(d), _ptr(s_), _ptr(found)))
+        return pd, pi, nl, rd, found
+
+    def set_join_inserts(self, mode):
+        """kg_set_join_inserts: 'auto', 'locked' or 'deferred'."""
+        self._check(self.L.kg_set_join_inserts(self.h, INSERTS[mode] if isinstance(mode, str) else int(mode)))
 
     def join_stats(self):
         st = JoinStats()

@@ -230,9 +230,29 @@ __global__ void __launch_bounds__(256) join_kernel(BuildState s) {
             const float rx = (valid && t == 0) ? *reinterpret_cast<volatile float *>(s.radius + x) : 0.f;
             const float ry = (valid && t == 1) ? *reinterpret_cast<volatile float *>(s.radius + y) : 0.f;
             const unsigned vm_all = __ballot_sync(FULL, valid && t == 0);
-            const unsigned nx = __ballot_sync(FULL, valid && t == 0 && !(dd > rx));
-            const unsigned ny = __ballot_sync(FULL, valid && t == 1 && !(dd > ry));
+            unsigned nx = __ballot_sync(FULL, valid && t == 0 && !(dd > rx));
+            unsigned ny = __ballot_sync(FULL, valid && t == 1 && !(dd > ry));
             comps += __popc(vm_all);
+            if (s.off_lin && (nx | ny)) {
+                // deferred: the offers go to the grouped merge after the join (one
+                // cursor atomic per pass); those beyond the buffer's capacity are
+                // inserted here under the lock
+                const unsigned om = nx | ny;
+                unsigned long long b0 = 0;
+                if (lane == 0) b0 = atomicAdd(s.off_cursor, (unsigned long long)__popc(om));
+                b0 = __shfl_sync(FULL, b0, 0);
+                const unsigned long long fit = b0 >= s.off_cap ? 0ull : s.off_cap - b0;
+                const uint32_t rank = __popc(om & ((1u << lane) - 1u));
+                const bool mine = ((om >> lane) & 1u) && rank < fit;
+                if (mine) {
+                    const uint32_t tg = t == 0 ? x : y;
+                    s.off_lin[b0 + rank] = make_uint4(tg, t == 0 ? y : x, __float_as_uint(dd), n | (t == 0 ? OFFER_UU : 0u));
+                    atomicAdd(s.off_cnt + tg, 1u);
+                }
+                const unsigned dm = __ballot_sync(FULL, mine);
+                nx &= ~dm;
+                ny &= ~dm;
+            }
             // only the pairs with an offer that passed a radius test: a pair both endpoints reject
             // inserts nothing and leaves r at pool.size() (>= K)
             unsigned vm = nx | (ny >> 1);
@@ -280,6 +300,223 @@ __global__ void __launch_bounds__(256) join_kernel(BuildState s) {
     if (lane == 0 && tally.attempts) {
         atomicAdd(s.inserts, tally.attempts);
         atomicAdd(s.inserts + 1, tally.landed);
+    }
+}
+
+// ------------------------------------------------------------------ deferred inserts
+// Offers of one join grouped by target: off_grp[off_pos[x] ..) holds x's.
+__global__ void offer_scatter_kernel(BuildState s) {
+    const unsigned long long total = min(*s.off_cursor, s.off_cap);
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const uint4 o = s.off_lin[i];
+        const uint32_t at = atomicAdd(s.off_fill + o.x, 1u);
+        s.off_grp[s.off_pos[o.x] + at] = o;
+    }
+}
+
+// Order-preserving map of a float's bits to an unsigned key, and back.
+__device__ __forceinline__ uint32_t f2ord(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ord2f(uint32_t u) { return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u); }
+
+constexpr uint32_t MG_CH = 512;     // offers merged per pass (sorted in shared memory)
+constexpr int MG_WARPS = 8;
+size_t merge_warp_bytes(uint32_t PS) { return (size_t)MG_CH * 24 + (size_t)PS * 16; }
+
+// Nhood::parallel_try_insert (kgraph.cpp:723-736) of every deferred offer
+// into its pool, one warp per pool, without locks (the join has finished).
+// A pool takes its offers in ascending (distance, id) order -- a serial order
+// the reference's threads can produce -- in passes of up to MG_CH, each pass
+// in one merge that reproduces the successive UpdateKnnListHelper calls
+// (kgraph.cpp:176-202):
+//  * an offer equal to an earlier one or to a pool entry (same id, same
+//    distance) is a duplicate;
+//  * the q-th non-duplicate lands at p = (pool entries <= d) + q, and every
+//    non-duplicate with p < L passes the radius test (the list's last entry
+//    then lies after it): these are a prefix of the non-duplicates;
+//  * the rest reach a full list: the first of them passes only against the
+//    stored radius, which an insert sets only when the list was already full
+//    (it may still be FLT_MAX), later ones only at a distance equal to the
+//    list's last entry; each lands in the overflow slot L, its duplicate test
+//    made against the list as it then is;
+//  * `found` of the offer's source node is set when an x <- y offer lands
+//    below K; L and the radius end as after the serial inserts.
+__global__ void __launch_bounds__(MG_WARPS * 32) offer_merge_kernel(BuildState s) {
+    extern __shared__ __align__(16) unsigned char mg_smem[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    unsigned char *wbase = mg_smem + (size_t)wib * s.mg_warp_bytes;
+    unsigned long long *keys = reinterpret_cast<unsigned long long *>(wbase);
+    uint32_t *vals = reinterpret_cast<uint32_t *>(keys + MG_CH);
+    uint32_t *paux = vals + MG_CH;                              // p of a non-duplicate, else ~0
+    uint32_t *qaux = paux + MG_CH;                              // its index among the non-duplicates
+    float *acc_d = reinterpret_cast<float *>(qaux + MG_CH);     // the accepted offers, in order
+    float *pdA = acc_d + MG_CH;
+    uint32_t *piA = reinterpret_cast<uint32_t *>(pdA + s.PS);
+    float *pdB = reinterpret_cast<float *>(piA + s.PS);
+    uint32_t *piB = reinterpret_cast<uint32_t *>(pdB + s.PS);
+    const uint32_t N = s.D.n, L = s.L, Lp = s.Lp;
+    unsigned long long att = 0, landed = 0;
+    for (;;) {
+        uint32_t x = 0;
+        if (lane == 0) x = atomicAdd(s.mg_work, 1u);
+        x = __shfl_sync(FULL, x, 0);
+        if (x >= N) break;
+        const uint32_t m = s.off_cnt[x];
+        if (m == 0) continue;
+        const uint64_t o0 = s.off_pos[x];
+        float *pd = pdA, *pdn = pdB;
+        uint32_t *pi = piA, *pin = piB;
+        float *gpd = s.pool_d + (size_t)x * s.PS;
+        uint32_t *gpi = s.pool_i + (size_t)x * s.PS;
+        for (uint32_t j = lane; j < Lp; j += 32) { pd[j] = gpd[j]; pi[j] = gpi[j]; }
+        uint32_t Lc = s.nodeL[x];
+        float rad = s.radius[x];
+        bool rad_set = false;
+        __syncwarp();
+        for (uint32_t c0 = 0; c0 < m; c0 += MG_CH) {
+            const uint32_t cm = min(MG_CH, m - c0);
+            uint32_t P2 = 32;
+            while (P2 < cm) P2 <<= 1;
+            for (uint32_t k = lane; k < P2; k += 32) {
+                unsigned long long key = ~0ull;
+                uint32_t v = 0;
+                if (k < cm) {
+                    const uint4 o = s.off_grp[o0 + c0 + k];
+                    key = ((unsigned long long)f2ord(__uint_as_float(o.z)) << 32) | o.y;
+                    v = o.w;
+                }
+                keys[k] = key;
+                vals[k] = v;
+            }
+            __syncwarp();
+            for (uint32_t kk = 2; kk <= P2; kk <<= 1) {   // bitonic sort, ascending (distance, id)
+                for (uint32_t jj = kk >> 1; jj > 0; jj >>= 1) {
+                    for (uint32_t i = lane; i < P2; i += 32) {
+                        const uint32_t ixj = i ^ jj;
+                        if (ixj > i) {
+                            const unsigned long long a = keys[i], b = keys[ixj];
+                            if ((a > b) == ((i & kk) == 0)) {
+                                keys[i] = b;
+                                keys[ixj] = a;
+                                const uint32_t t = vals[i];
+                                vals[i] = vals[ixj];
+                                vals[ixj] = t;
+                            }
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+            // positions of the non-duplicates
+            uint32_t nnd = 0;
+            for (uint32_t k0 = 0; k0 < cm; k0 += 32) {
+                const uint32_t k = k0 + lane;
+                bool nd = false;
+                uint32_t rk = 0;
+                if (k < cm) {
+                    const unsigned long long key = keys[k];
+                    const float d = ord2f((uint32_t)(key >> 32));
+                    const uint32_t c = (uint32_t)key;
+                    bool dup = k > 0 && keys[k - 1] == key;
+                    uint32_t lo = 0, hi = Lc;   // pool entries <= d
+                    while (lo < hi) {
+                        const uint32_t mid = (lo + hi) >> 1;
+                        if (pd[mid] <= d) lo = mid + 1; else hi = mid;
+                    }
+                    rk = lo;
+                    for (int j = (int)rk - 1; !dup && j >= 0 && pd[j] == d; --j) dup = (pi[j] & ID_MASK) == c;
+                    nd = !dup;
+                }
+                const unsigned ndm = __ballot_sync(FULL, nd);
+                const uint32_t q = nnd + __popc(ndm & ((1u << lane) - 1u));
+                if (k < cm) {
+                    paux[k] = nd ? rk + q : 0xFFFFFFFFu;
+                    qaux[k] = q;
+                }
+                nnd += __popc(ndm);
+            }
+            __syncwarp();
+            // the main inserts (p < L), in order; `found` of their sources
+            uint32_t qs = 0;
+            for (uint32_t k = lane; k < cm; k += 32) {
+                const uint32_t p = paux[k];
+                if (p < L) {
+                    ++qs;
+                    acc_d[qaux[k]] = ord2f((uint32_t)(keys[k] >> 32));
+                    const uint32_t v = vals[k];
+                    if ((v & OFFER_UU) && p < s.K) s.found[v & ~OFFER_UU] = 1u;
+                }
+            }
+            for (int o = 16; o; o >>= 1) qs += __shfl_xor_sync(FULL, qs, o);
+            for (uint32_t j = lane; j < Lp; j += 32) { pdn[j] = pd[j]; pin[j] = pi[j]; }
+            __syncwarp();
+            for (uint32_t j = lane; j < Lc; j += 32) {   // pool entries move up past the accepted offers below them
+                const float dj = pd[j];
+                uint32_t lo = 0, hi = qs;
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (acc_d[mid] < dj) lo = mid + 1; else hi = mid;
+                }
+                const uint32_t np = j + lo;
+                if (np < Lp) { pdn[np] = dj; pin[np] = pi[j]; }
+            }
+            __syncwarp();
+            for (uint32_t k = lane; k < cm; k += 32) {
+                const uint32_t p = paux[k];
+                if (p < L) { pdn[p] = ord2f((uint32_t)(keys[k] >> 32)); pin[p] = (uint32_t)keys[k] | FLAG_BIT; }
+            }
+            __syncwarp();
+            const bool full_main = qs + Lc > L;   // an insert reached a full list
+            uint32_t ntail = 0;
+            if (Lc + qs >= L && lane == 0) {
+                // the offers beyond the list, in order (lane 0; a short run: at most one offer
+                // above the list's last distance can land)
+                const float dL = pdn[L - 1];
+                float rc = full_main ? dL : rad;
+                // first offer at or above dL that is not a main insert
+                uint32_t lo = 0, hi = cm;
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (ord2f((uint32_t)(keys[mid] >> 32)) < dL) lo = mid + 1; else hi = mid;
+                }
+                for (uint32_t k = lo; k < cm; ++k) {
+                    if (paux[k] < L) continue;
+                    const float d = ord2f((uint32_t)(keys[k] >> 32));
+                    if (d > rc) break;
+                    const uint32_t c = (uint32_t)keys[k];
+                    bool dup = false;
+                    for (int j = (int)L - 1; !dup && j >= 0 && pdn[j] == d; --j) dup = (pin[j] & ID_MASK) == c;
+                    if (dup) continue;
+                    pdn[L] = d;
+                    pin[L] = c | FLAG_BIT;
+                    rc = dL;
+                    ++ntail;
+                }
+            }
+            ntail = __shfl_sync(FULL, ntail, 0);
+            __syncwarp();
+            // counts: offers that passed the radius test (duplicates included), and those that landed
+            att += (cm - nnd) + qs + ntail;
+            landed += qs + ntail;
+            if (full_main || ntail) { rad = pdn[L - 1]; rad_set = true; }
+            Lc = min(L, Lc + qs);
+            float *tf = pd; pd = pdn; pdn = tf;
+            uint32_t *ti = pi; pi = pin; pin = ti;
+            __syncwarp();
+        }
+        for (uint32_t j = lane; j < Lp; j += 32) { gpd[j] = pd[j]; gpi[j] = pi[j]; }
+        if (lane == 0) {
+            s.nodeL[x] = Lc;
+            if (rad_set) s.radius[x] = rad;
+        }
+        __syncwarp();
+    }
+    if (lane == 0 && att) {   // warp-uniform counts
+        atomicAdd(s.inserts, att);
+        atomicAdd(s.inserts + 1, landed);
     }
 }
 
@@ -695,6 +932,40 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
     cudaMemsetAsync(s.rcnt_new + N, 0, 4, st);   // scan inputs carry one extra zero
     cudaMemsetAsync(s.rcnt_old + N, 0, 4, st);
 
+    // Deferred inserts of the FP32 join: the offer records (linear and grouped,
+    // 16 bytes each) hold up to 1024 offers per node within 30 % of the free
+    // device memory and 20 GB; the per-target counts, cursors and offsets.
+    size_t offer_scan_bytes = 0;
+    s.mg_warp_bytes = (uint32_t)merge_warp_bytes(s.PS);
+    const int mg_warps = (int)std::min<size_t>(MG_WARPS, (227u << 10) / s.mg_warp_bytes);
+    if (ctx->join_inserts != KG_INSERTS_LOCKED && mg_warps >= 1) {
+        size_t freeb = 0, totalb = 0;
+        cudaMemGetInfo(&freeb, &totalb);
+        const size_t own = ctx->offer_lin.bytes + ctx->offer_grp.bytes;
+        size_t cap = std::min<size_t>((size_t)20 << 30, (freeb + own) / 10 * 3) / 32;
+        cap = std::min<size_t>(cap, n * 1024);
+        if (cap >= 1024) {
+            if ((e = ctx->offer_lin.reserve(cap * 16)) != cudaSuccess || (e = ctx->offer_grp.reserve(cap * 16)) != cudaSuccess ||
+                (e = ctx->offer_aux.reserve((n + 1) * 8 + (n + 1) * 4 + n * 4 + 16)) != cudaSuccess)
+                return cuda_fail(ctx, e, "alloc join offers");
+            s.off_lin = ctx->offer_lin.as<uint4>();
+            s.off_grp = ctx->offer_grp.as<uint4>();
+            s.off_cap = cap;
+            s.off_pos = ctx->offer_aux.as<uint64_t>();
+            s.off_cnt = reinterpret_cast<uint32_t *>(s.off_pos + n + 1);
+            s.off_fill = s.off_cnt + n + 1;
+            s.off_cursor = s.n_comps + 9;                                  // in the counter block
+            s.mg_work = reinterpret_cast<uint32_t *>(s.n_comps + 10);
+            cub::DeviceScan::ExclusiveSum(nullptr, offer_scan_bytes, s.off_cnt, s.off_pos, N + 1, st);
+            if ((e = ctx->offer_scan.reserve(offer_scan_bytes)) != cudaSuccess) return cuda_fail(ctx, e, "alloc join offers");
+            const size_t mg_smem = (size_t)mg_warps * s.mg_warp_bytes;
+            if (mg_smem > 48 * 1024 &&
+                (e = cudaFuncSetAttribute(offer_merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mg_smem)) !=
+                    cudaSuccess)
+                return cuda_fail(ctx, e, "join merge");
+        }
+    }
+
     // GenerateControl (kgraph.cpp:254-270): C distinct random nodes, exact K-NN.
     if (g_verbosity > 0) std::cerr << "Generating control..." << std::endl;
     std::vector<uint32_t> hctrl(C);
@@ -754,7 +1025,20 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
     // the statistics with their copies to the host, and the update.
     auto rec_join = [&]() -> cudaError_t {
         cudaMemsetAsync(s.work, 0, 4, st);
+        if (s.off_lin) {
+            cudaMemsetAsync(s.off_cursor, 0, 16, st);   // the offer cursor and the merge's claim counter
+            cudaMemsetAsync(s.off_cnt, 0, (n + 1) * 4, st);
+            cudaMemsetAsync(s.off_fill, 0, n * 4, st);
+        }
         join_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
+        if (s.off_lin) {
+            size_t sb = offer_scan_bytes;
+            cudaError_t e2 = cub::DeviceScan::ExclusiveSum(ctx->offer_scan.p, sb, s.off_cnt, s.off_pos, N + 1, st);
+            if (e2 != cudaSuccess) return e2;
+            offer_scatter_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
+            const int bps = std::max(1, (int)((228u << 10) / ((size_t)mg_warps * s.mg_warp_bytes + 1024)));
+            offer_merge_kernel<<<ctx->num_sms * bps, mg_warps * 32, (size_t)mg_warps * s.mg_warp_bytes, st>>>(s);
+        }
         return cudaGetLastError();
     };
     auto rec_stats = [&]() -> cudaError_t {
@@ -1001,6 +1285,98 @@ extern "C" int kg_set_join_precision(kg_ctx *ctx, int mode) {
     if (!ctx || mode < KG_JOIN_AUTO || mode > KG_JOIN_FP8_ALWAYS) return KG_E_INVALID;
     std::lock_guard<std::mutex> guard(ctx->mu);
     ctx->join_mode = mode;
+    return KG_OK;
+}
+
+// The deferred-insert merge (offer_scatter_kernel + offer_merge_kernel) on
+// caller data: n pools of Lp = L+1 entries (host rows of Lp, ids with the new
+// flag in bit 31), their list lengths and radii (in/out), and n_off offers
+// (target, candidate, distance, source | OFFER_UU); found[src] (out) is set as
+// in the join.  For tests of the merge against serial inserts.
+extern "C" int kg_join_merge_check(kg_ctx *ctx, unsigned n, unsigned L, unsigned K, float *pool_d, uint32_t *pool_i,
+                                   uint32_t *nodeL, float *radius, size_t n_off, const uint32_t *target,
+                                   const uint32_t *cand, const float *dist, const uint32_t *src, uint32_t *found) {
+    if (!ctx) return KG_E_INVALID;
+    std::lock_guard<std::mutex> guard(ctx->mu);
+    cudaSetDevice(ctx->device);
+    if (n == 0 || L == 0 || K > L || !pool_d || !pool_i || !nodeL || !radius || !found || (n_off && (!target || !cand || !dist || !src)))
+        return set_error(ctx, KG_E_INVALID, "bad merge check arguments");
+    for (size_t k = 0; k < n_off; ++k)
+        if (target[k] >= n || (src[k] & ~OFFER_UU) >= n) return set_error(ctx, KG_E_INVALID, "offer node out of range");
+    BuildState s{};
+    s.L = L; s.Lp = L + 1; s.K = K;
+    s.PS = (s.Lp + 7) / 8 * 8;
+    s.D.n = n;
+    s.mg_warp_bytes = (uint32_t)merge_warp_bytes(s.PS);
+    const int mg_warps = (int)std::min<size_t>(MG_WARPS, (227u << 10) / s.mg_warp_bytes);
+    if (mg_warps < 1) return set_error(ctx, KG_E_INVALID, "L too large for the merge");
+    std::vector<float> hd((size_t)n * s.PS, FLT_MAX);
+    std::vector<uint32_t> hi((size_t)n * s.PS, UNSET_ID), cnt(n + 1, 0);
+    for (size_t x = 0; x < n; ++x)
+        for (uint32_t j = 0; j < s.Lp; ++j) { hd[x * s.PS + j] = pool_d[x * s.Lp + j]; hi[x * s.PS + j] = pool_i[x * s.Lp + j]; }
+    std::vector<uint4> lin(std::max<size_t>(n_off, 1));
+    for (size_t k = 0; k < n_off; ++k) {
+        uint32_t db;
+        std::memcpy(&db, &dist[k], 4);
+        lin[k] = make_uint4(target[k], cand[k], db, src[k]);
+        ++cnt[target[k]];
+    }
+    DevBuf b[10];
+    cudaError_t e;
+    const size_t rows = (size_t)n * s.PS;
+    size_t scan_bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (uint32_t *)nullptr, (uint64_t *)nullptr, n + 1, ctx->stream);
+    if ((e = b[0].reserve(rows * 4)) != cudaSuccess || (e = b[1].reserve(rows * 4)) != cudaSuccess ||
+        (e = b[2].reserve((size_t)n * 4)) != cudaSuccess || (e = b[3].reserve((size_t)n * 4)) != cudaSuccess ||
+        (e = b[4].reserve((size_t)n * 4)) != cudaSuccess || (e = b[5].reserve(lin.size() * 16)) != cudaSuccess ||
+        (e = b[6].reserve(lin.size() * 16)) != cudaSuccess || (e = b[7].reserve((size_t)(n + 1) * 12 + (size_t)n * 4)) != cudaSuccess ||
+        (e = b[8].reserve(64)) != cudaSuccess || (e = b[9].reserve(scan_bytes)) != cudaSuccess)
+        return cuda_fail(ctx, e, "alloc merge check");
+    s.pool_d = b[0].as<float>(); s.pool_i = b[1].as<uint32_t>();
+    s.nodeL = b[2].as<uint32_t>(); s.radius = b[3].as<float>(); s.found = b[4].as<uint32_t>();
+    s.off_lin = b[5].as<uint4>(); s.off_grp = b[6].as<uint4>();
+    s.off_pos = b[7].as<uint64_t>();
+    s.off_cnt = reinterpret_cast<uint32_t *>(s.off_pos + n + 1);
+    s.off_fill = s.off_cnt + n + 1;
+    s.off_cursor = b[8].as<unsigned long long>();
+    s.mg_work = reinterpret_cast<uint32_t *>(s.off_cursor + 1);
+    s.inserts = s.off_cursor + 2;
+    s.off_cap = n_off;
+    cudaStream_t st = ctx->stream;
+    const unsigned long long head[4] = {n_off, 0, 0, 0};
+    cudaMemcpyAsync(s.pool_d, hd.data(), rows * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(s.pool_i, hi.data(), rows * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(s.nodeL, nodeL, (size_t)n * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(s.radius, radius, (size_t)n * 4, cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(s.found, 0, (size_t)n * 4, st);
+    cudaMemcpyAsync(s.off_lin, lin.data(), lin.size() * 16, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(s.off_cnt, cnt.data(), (size_t)(n + 1) * 4, cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(s.off_fill, 0, (size_t)n * 4, st);
+    cudaMemcpyAsync(s.off_cursor, head, sizeof(head), cudaMemcpyHostToDevice, st);
+    if ((e = cub::DeviceScan::ExclusiveSum(b[9].p, scan_bytes, s.off_cnt, s.off_pos, n + 1, st)) != cudaSuccess)
+        return cuda_fail(ctx, e, "merge check scan");
+    offer_scatter_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
+    const size_t mg_smem = (size_t)mg_warps * s.mg_warp_bytes;
+    if (mg_smem > 48 * 1024 &&
+        (e = cudaFuncSetAttribute(offer_merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mg_smem)) != cudaSuccess)
+        return cuda_fail(ctx, e, "merge check");
+    offer_merge_kernel<<<ctx->num_sms, mg_warps * 32, mg_smem, st>>>(s);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "merge check launch");
+    cudaMemcpyAsync(hd.data(), s.pool_d, rows * 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hi.data(), s.pool_i, rows * 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(nodeL, s.nodeL, (size_t)n * 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(radius, s.radius, (size_t)n * 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(found, s.found, (size_t)n * 4, cudaMemcpyDeviceToHost, st);
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "merge check");
+    for (size_t x = 0; x < n; ++x)
+        for (uint32_t j = 0; j < s.Lp; ++j) { pool_d[x * s.Lp + j] = hd[x * s.PS + j]; pool_i[x * s.Lp + j] = hi[x * s.PS + j]; }
+    return KG_OK;
+}
+
+extern "C" int kg_set_join_inserts(kg_ctx *ctx, int mode) {
+    if (!ctx || mode < KG_INSERTS_AUTO || mode > KG_INSERTS_DEFERRED) return KG_E_INVALID;
+    std::lock_guard<std::mutex> guard(ctx->mu);
+    ctx->join_inserts = mode;
     return KG_OK;
 }
 

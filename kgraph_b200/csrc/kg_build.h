@@ -34,7 +34,22 @@ struct BuildState {
     uint32_t *iter;                      // iteration number, advanced on the device
                                          // so that one captured graph serves every iteration
     struct JoinTcStats *tc;              // tensor-core join counters (kg_join_tc.cu)
+    // Deferred inserts of the FP32 join (null off_lin: every insert is locked).
+    // The join appends each offer that passes the unlocked radius test to
+    // off_lin ({target, candidate, distance bits, source node | OFFER_UU}) while
+    // off_cursor stays below off_cap (the excess takes the locked path) and
+    // counts it in off_cnt[target]; the offers are then grouped by target into
+    // off_grp (off_pos: exclusive scan of off_cnt; off_fill: cursors) and each
+    // pool takes its offers in one merge (offer_merge_kernel).
+    uint4 *off_lin, *off_grp;
+    unsigned long long *off_cursor, off_cap;
+    uint32_t *off_cnt, *off_fill, *mg_work;
+    uint64_t *off_pos;
+    uint32_t mg_warp_bytes;              // shared memory per merging warp
 };
+// Source-node word of a deferred offer: set when the offer is the pair's
+// x <- y insert, whose position decides the source node's `found`.
+constexpr uint32_t OFFER_UU = 0x80000000u;
 
 // Counters of the tensor-core join, accumulated over a build.  Errors are of
 // the BF16 tile distance against an FP64 evaluation of the same pair, on a

@@ -163,6 +163,7 @@ void kg_ctx_destroy(kg_ctx *c) {
     DevBuf *bufs[] = {&c->X, &c->norms, &c->offsets, &c->nbr, &c->nbr_d, &c->Mnode, &c->errw, &c->counter, &c->ell, &c->meta,
                       &c->visited, &c->qbuf, &c->kbuf, &c->pbuf, &c->seeds, &c->seed_index, &c->init_ids,
                       &c->out_ids, &c->out_d, &c->out_cnt, &c->out_cost, &c->tcstat, &c->joinq, &c->joinaux, &c->joinb,
+                      &c->offer_lin, &c->offer_grp, &c->offer_aux, &c->offer_scan,
                       &c->Xc, &c->cmeta, &c->cstats, &c->bf_rows, &c->bf_meta, &c->bf_aux, &c->bf_work};
     for (DevBuf *b : bufs) b->release();
     for (auto &b : c->build_scratch) b.release();

@@ -92,6 +92,8 @@ struct kg_ctx {
     int join_mode = KG_JOIN_AUTO;
     kgb::DevBuf tcstat;              // tensor-core join counters
     kgb::DevBuf joinq, joinaux, joinb;   // tensor-core join: candidate queue, worst-case prefix, round bounds
+    kgb::DevBuf offer_lin, offer_grp, offer_aux, offer_scan;   // deferred join inserts (kg_build.cu)
+    int join_inserts = KG_INSERTS_AUTO;
     kg_join_stats last_join{};
     // tensor-core brute force (kg_bruteforce.cu): BF16 centred rows, row terms, mean + extents, work space
     kgb::DevBuf bf_rows, bf_meta, bf_aux, bf_work;

@@ -671,4 +671,21 @@ uint64_t kgo_prune(unsigned n, const uint64_t *offsets, const uint32_t *ids, con
     return store_result(std::move(g));
 }
 
+void kgo_serial_inserts(unsigned Lp, float *pool_d, uint32_t *pool_i, unsigned *L, float *radius, unsigned n_off,
+                        const uint32_t *cand, const float *dist, uint32_t *r_out) {
+    Nhood nh;
+    nh.pool.resize(Lp);
+    for (unsigned j = 0; j < Lp; ++j)
+        nh.pool[j] = Neighbor{pool_i[j] & 0x7FFFFFFFu, pool_d[j], (pool_i[j] & 0x80000000u) != 0};
+    nh.L = *L;
+    nh.radius = *radius;
+    for (unsigned k = 0; k < n_off; ++k) r_out[k] = nh.try_insert(cand[k], dist[k]);
+    for (unsigned j = 0; j < Lp; ++j) {
+        pool_d[j] = nh.pool[j].dist;
+        pool_i[j] = nh.pool[j].id | (nh.pool[j].flag ? 0x80000000u : 0u);
+    }
+    *L = nh.L;
+    *radius = nh.radius;
+}
+
 }  // extern "C"

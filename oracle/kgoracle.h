@@ -97,6 +97,14 @@ uint64_t kgo_reverse(unsigned n, const uint64_t *offsets, const uint32_t *ids, c
 uint64_t kgo_prune(unsigned n, const uint64_t *offsets, const uint32_t *ids, const float *dists,
                    const uint32_t *M, unsigned level);
 
+/* Nhood::parallel_try_insert (kgraph.cpp:723-736) of n_off offers (cand[k],
+ * dist[k]) in the given order into one pool of Lp = L+1 entries (ids with the
+ * new-flag in bit 31), its list length *L and *radius; r_out[k] = the
+ * reference's return value (pool.size() for a radius rejection, L+1 for a
+ * duplicate, else the insert position). */
+void kgo_serial_inserts(unsigned Lp, float *pool_d, uint32_t *pool_i, unsigned *L, float *radius, unsigned n_off,
+                        const uint32_t *cand, const float *dist, uint32_t *r_out);
+
 /* libstdc++ std::sort by dist on (dist, id) pairs -- what the reference's
  * sort(pool) / sort(knn) calls do (kgraph.cpp:476, 697, 793). */
 void kgo_std_sort_pairs(float *dists, uint32_t *ids, unsigned n);

@@ -56,6 +56,8 @@ def _lib():
     lib.kgo_prune.restype = C.c_uint64
     lib.kgo_prune.argtypes = [u, _u64p, _u32p, _f32p, _u32p, u]
     lib.kgo_std_sort_pairs.argtypes = [_f32p, _u32p, u]
+    lib.kgo_serial_inserts.argtypes = [u, _f32p, _u32p, C.POINTER(C.c_uint), C.POINTER(C.c_float), u, _u32p, _f32p,
+                                       _u32p]
     lib.kgo_last_error.restype = C.c_char_p
     return lib
 
@@ -169,6 +171,20 @@ def genrandom(seed, size, N, calls=0):
     out = np.zeros(max(size, 1), np.uint32)
     _lib().kgo_genrandom(seed, size, N, calls, out)
     return out[:size]
+
+
+def serial_inserts(pool_d, pool_i, L, radius, cand, dist):
+    """Nhood::parallel_try_insert of the offers (cand[k], dist[k]) in order into
+    one pool (Lp = len(pool_d) entries, ids with the new-flag in bit 31).
+    Returns (pool_d, pool_i, L, radius, r)."""
+    pd = np.ascontiguousarray(pool_d, np.float32).copy()
+    pi = np.ascontiguousarray(pool_i, np.uint32).copy()
+    c = np.ascontiguousarray(cand, np.uint32)
+    d = np.ascontiguousarray(dist, np.float32)
+    r = np.zeros(len(c), np.uint32)
+    Lv, rv = C.c_uint(int(L)), C.c_float(float(radius))
+    _lib().kgo_serial_inserts(len(pd), pd, pi, C.byref(Lv), C.byref(rv), len(c), c, d, r)
+    return pd, pi, Lv.value, rv.value, r
 
 
 def std_sort_pairs(dists, ids):
