@@ -205,6 +205,57 @@ __device__ __forceinline__ void pair_dist_shared(const DataView &D, uint32_t j, 
 }
 
 // ------------------------------------------------------------------ join
+// One pass of 8 pairs (one per 4-lane group: lanes 4p..4p+3 hold pair p's
+// x, y and distance, valid marking a pair to evaluate; node n's join made
+// them): the unlocked radius pre-test for both directions (kgraph.cpp:725),
+// then Nhood::parallel_try_insert of the offers that passed -- recorded for
+// the deferred merge while the record buffer has room, else under the
+// target's lock here.  uu is set when an x <- y insert lands below K
+// (kgraph.cpp:808-810); comps counts the pairs (the reference's cc).
+__device__ __forceinline__ void settle_pass(const BuildState &s, int lane, int t, bool valid, uint32_t x, uint32_t y,
+                                            float dd, uint32_t n, unsigned long long &comps, bool &uu,
+                                            InsertTally &tally) {
+    const float rx = (valid && t == 0) ? *reinterpret_cast<volatile float *>(s.radius + x) : 0.f;
+    const float ry = (valid && t == 1) ? *reinterpret_cast<volatile float *>(s.radius + y) : 0.f;
+    const unsigned vm_all = __ballot_sync(FULL, valid && t == 0);
+    unsigned nx = __ballot_sync(FULL, valid && t == 0 && !(dd > rx));
+    unsigned ny = __ballot_sync(FULL, valid && t == 1 && !(dd > ry));
+    comps += __popc(vm_all);
+    if (s.off_lin && (nx | ny)) {
+        // deferred: the offers go to the grouped merge after the join (one
+        // cursor atomic per pass); those beyond the buffer's capacity are
+        // inserted here under the lock
+        const unsigned om = nx | ny;
+        unsigned long long b0 = 0;
+        if (lane == 0) b0 = atomicAdd(s.off_cursor, (unsigned long long)__popc(om));
+        b0 = __shfl_sync(FULL, b0, 0);
+        const unsigned long long fit = b0 >= s.off_cap ? 0ull : s.off_cap - b0;
+        const uint32_t rank = __popc(om & ((1u << lane) - 1u));
+        const bool mine = ((om >> lane) & 1u) && rank < fit;
+        if (mine) {
+            const uint32_t tg = t == 0 ? x : y;
+            s.off_lin[b0 + rank] = make_uint4(tg, t == 0 ? y : x, __float_as_uint(dd), n | (t == 0 ? OFFER_UU : 0u));
+            atomicAdd(s.off_cnt + tg, 1u);
+        }
+        const unsigned dm = __ballot_sync(FULL, mine);
+        nx &= ~dm;
+        ny &= ~dm;
+    }
+    // only the pairs with an offer that passed a radius test: a pair both endpoints reject
+    // inserts nothing and leaves r at pool.size() (>= K)
+    unsigned vm = nx | (ny >> 1);
+    while (vm) {
+        const int src = __ffs(vm) - 1;
+        vm &= vm - 1;
+        const uint32_t xg = __shfl_sync(FULL, x, src), yg = __shfl_sync(FULL, y, src);
+        const float dg = __shfl_sync(FULL, dd, src);
+        uint32_t r = s.Lp;
+        if (nx & (1u << src)) r = locked_insert(s, xg, yg, dg, lane, tally);
+        if (r < s.K) uu = true;
+        if (ny & (1u << (src + 1))) locked_insert(s, yg, xg, dg, lane, tally);
+    }
+}
+
 // KGraphConstructor::join + Nhood::join (kgraph.cpp:740-751, 797-815).  The
 // node's new entries are taken two at a time: the second one's partners are
 // the first one's minus the second itself, so each partner row read serves
@@ -224,48 +275,8 @@ __global__ void __launch_bounds__(256) join_kernel(BuildState s) {
         const uint32_t *nw = s.nn_new + (size_t)n * s.NEWCAP;
         const uint32_t *od = s.nn_old + (size_t)n * s.OLDCAP;
         bool uu = false;
-        // One pair per 4-lane group: the unlocked radius pre-test for both
-        // directions, then Nhood::parallel_try_insert of the group's pairs in turn.
         auto settle = [&](bool valid, uint32_t x, uint32_t y, float dd) {
-            const float rx = (valid && t == 0) ? *reinterpret_cast<volatile float *>(s.radius + x) : 0.f;
-            const float ry = (valid && t == 1) ? *reinterpret_cast<volatile float *>(s.radius + y) : 0.f;
-            const unsigned vm_all = __ballot_sync(FULL, valid && t == 0);
-            unsigned nx = __ballot_sync(FULL, valid && t == 0 && !(dd > rx));
-            unsigned ny = __ballot_sync(FULL, valid && t == 1 && !(dd > ry));
-            comps += __popc(vm_all);
-            if (s.off_lin && (nx | ny)) {
-                // deferred: the offers go to the grouped merge after the join (one
-                // cursor atomic per pass); those beyond the buffer's capacity are
-                // inserted here under the lock
-                const unsigned om = nx | ny;
-                unsigned long long b0 = 0;
-                if (lane == 0) b0 = atomicAdd(s.off_cursor, (unsigned long long)__popc(om));
-                b0 = __shfl_sync(FULL, b0, 0);
-                const unsigned long long fit = b0 >= s.off_cap ? 0ull : s.off_cap - b0;
-                const uint32_t rank = __popc(om & ((1u << lane) - 1u));
-                const bool mine = ((om >> lane) & 1u) && rank < fit;
-                if (mine) {
-                    const uint32_t tg = t == 0 ? x : y;
-                    s.off_lin[b0 + rank] = make_uint4(tg, t == 0 ? y : x, __float_as_uint(dd), n | (t == 0 ? OFFER_UU : 0u));
-                    atomicAdd(s.off_cnt + tg, 1u);
-                }
-                const unsigned dm = __ballot_sync(FULL, mine);
-                nx &= ~dm;
-                ny &= ~dm;
-            }
-            // only the pairs with an offer that passed a radius test: a pair both endpoints reject
-            // inserts nothing and leaves r at pool.size() (>= K)
-            unsigned vm = nx | (ny >> 1);
-            while (vm) {
-                const int src = __ffs(vm) - 1;
-                vm &= vm - 1;
-                const uint32_t xg = __shfl_sync(FULL, x, src), yg = __shfl_sync(FULL, y, src);
-                const float dg = __shfl_sync(FULL, dd, src);
-                uint32_t r = s.Lp;
-                if (nx & (1u << src)) r = locked_insert(s, xg, yg, dg, lane, tally);
-                if (r < s.K) uu = true;
-                if (ny & (1u << (src + 1))) locked_insert(s, yg, xg, dg, lane, tally);
-            }
+            settle_pass(s, lane, t, valid, x, y, dd, n, comps, uu, tally);
         };
         for (uint32_t ii = 0; ii < a; ii += 2) {
             const bool two = ii + 1 < a;
@@ -295,6 +306,86 @@ __global__ void __launch_bounds__(256) join_kernel(BuildState s) {
             }
         }
         if (lane == 0) s.found[n] = uu ? 1u : 0u;
+    }
+    if (lane == 0 && comps) atomicAdd(s.n_comps, comps);
+    if (lane == 0 && tally.attempts) {
+        atomicAdd(s.inserts, tally.attempts);
+        atomicAdd(s.inserts + 1, tally.landed);
+    }
+}
+
+// The same join with a node's lists staged in shared memory: one CTA per node
+// copies the rows of new ++ old (jt_rows of them; rows beyond are read from
+// global memory) and their norm terms once, then evaluates the node's pairs
+// from there -- each 4-lane group one pair per pass with the canonical
+// arithmetic (group4_raw, the same bits as pair_dist) -- so a node's partner
+// rows cross from L2/DRAM once per node instead of once per pair.  Pairs: for
+// new entry i (warp-strided), new[i+1 ..) then old, as join_kernel.
+constexpr int JT_WARPS = 4;
+__global__ void __launch_bounds__(JT_WARPS * 32) join_tile_kernel(BuildState s) {
+    extern __shared__ __align__(16) float jt_smem[];
+    __shared__ uint32_t s_node, s_uu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const uint32_t N = s.D.n, stride = s.D.ld + 4;   // 16 bytes of padding: rows start on different banks
+    const int metric = s.D.metric;
+    float *rows = jt_smem;
+    float *nrm = rows + (size_t)s.jt_rows * stride;
+    uint32_t *uid = reinterpret_cast<uint32_t *>(nrm + s.NEWCAP + s.OLDCAP);
+    unsigned long long comps = 0;
+    InsertTally tally;
+    for (;;) {
+        if (threadIdx.x == 0) { s_node = atomicAdd(s.work, 1u); s_uu = 0; }
+        __syncthreads();
+        const uint32_t n = s_node;
+        if (n >= N) break;
+        const uint32_t a = min(s.cnt_new[n], s.NEWCAP), b = min(s.cnt_old[n], s.OLDCAP);
+        if (a == 0) {
+            if (threadIdx.x == 0) s.found[n] = 0u;
+            __syncthreads();
+            continue;
+        }
+        const uint32_t U = a + b;
+        const uint32_t *nw = s.nn_new + (size_t)n * s.NEWCAP, *od = s.nn_old + (size_t)n * s.OLDCAP;
+        for (uint32_t u = threadIdx.x; u < U; u += blockDim.x) {
+            uint32_t id = u < a ? nw[u] : od[u - a];
+            if (id >= N) { raise_error(s.err, ERR_BAD_ID); id = NO_ID; }
+            uid[u] = id;
+            nrm[u] = (id != NO_ID && metric != METRIC_L2SQR) ? s.D.norms[id] : 0.f;
+        }
+        __syncthreads();
+        const uint32_t staged = min(U, s.jt_rows);
+        for (uint32_t r = warp; r < staged; r += JT_WARPS) {
+            const uint32_t id = uid[r] == NO_ID ? 0u : uid[r];
+            const float *src = s.D.X + (size_t)id * s.D.ld;
+            float *dst = rows + (size_t)r * stride;
+            for (uint32_t k = 4 * lane; k < s.D.ld; k += 128) *reinterpret_cast<float4 *>(dst + k) = ld4(src + k);
+        }
+        __syncthreads();
+        bool uu = false;
+        for (uint32_t i = warp; i < a; i += JT_WARPS) {
+            const uint32_t idi = uid[i];
+            const float *ri = i < s.jt_rows ? rows + (size_t)i * stride : s.D.X + (size_t)(idi == NO_ID ? 0u : idi) * s.D.ld;
+            const float ni = nrm[i];
+            const uint32_t nnn = a - 1 - i, inner = nnn + b;   // partners: new[i+1..a) then old
+            for (uint32_t base = 0; base < inner; base += 8) {
+                const uint32_t k = base + g;
+                const bool in = k < inner;
+                const uint32_t u = in ? (k < nnn ? i + 1 + k : a + (k - nnn)) : i;
+                const bool is_nn = u < a;
+                const uint32_t jid = uid[u];
+                // i < j by id excludes equal ids among the new entries (kgraph.cpp:742-743)
+                const bool v = in && idi != NO_ID && jid != NO_ID && !(is_nn && jid == idi);
+                const float *rj = u < s.jt_rows ? rows + (size_t)u * stride : s.D.X + (size_t)(jid == NO_ID ? 0u : jid) * s.D.ld;
+                const float raw = group4_raw(ri, rj, (int)s.D.d, metric, t, FULL);
+                const float dd = metric == METRIC_L2SQR ? raw : finish_metric(raw, ni, nrm[u], metric);
+                settle_pass(s, lane, t, v, v ? (is_nn ? min(idi, jid) : idi) : 0u, v ? (is_nn ? max(idi, jid) : jid) : 0u,
+                            dd, n, comps, uu, tally);
+            }
+        }
+        if (uu && lane == 0) atomicOr(&s_uu, 1u);
+        __syncthreads();
+        if (threadIdx.x == 0) s.found[n] = s_uu;
     }
     if (lane == 0 && comps) atomicAdd(s.n_comps, comps);
     if (lane == 0 && tally.attempts) {
@@ -932,6 +1023,21 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
     cudaMemsetAsync(s.rcnt_new + N, 0, 4, st);   // scan inputs carry one extra zero
     cudaMemsetAsync(s.rcnt_old + N, 0, 4, st);
 
+    // The shared-memory join: rows of new ++ old per node within 48 KB per CTA
+    // (4 CTAs per SM), the ids and norm terms beside them.
+    size_t jt_smem = 0;
+    int jt_blocks = 0;
+    s.jt_rows = 0;
+    if (ctx->join_tile) {
+        const size_t fixed = (size_t)(s.NEWCAP + s.OLDCAP) * 8;
+        const size_t row_bytes = (size_t)(s.D.ld + 4) * 4;
+        const size_t budget = 48 * 1024 - 64;
+        if (budget > fixed + 8 * row_bytes) {
+            s.jt_rows = (uint32_t)std::min<size_t>((budget - fixed) / row_bytes, s.NEWCAP + s.OLDCAP);
+            jt_smem = fixed + (size_t)s.jt_rows * row_bytes;
+            jt_blocks = 4;
+        }
+    }
     // Deferred inserts of the FP32 join: the offer records (linear and grouped,
     // 16 bytes each) hold up to 1024 offers per node within 30 % of the free
     // device memory and 20 GB; the per-target counts, cursors and offsets.
@@ -1030,7 +1136,10 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
             cudaMemsetAsync(s.off_cnt, 0, (n + 1) * 4, st);
             cudaMemsetAsync(s.off_fill, 0, n * 4, st);
         }
-        join_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
+        if (s.jt_rows)
+            join_tile_kernel<<<ctx->num_sms * jt_blocks, JT_WARPS * 32, jt_smem, st>>>(s);
+        else
+            join_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
         if (s.off_lin) {
             size_t sb = offer_scan_bytes;
             cudaError_t e2 = cub::DeviceScan::ExclusiveSum(ctx->offer_scan.p, sb, s.off_cnt, s.off_pos, N + 1, st);

@@ -46,6 +46,7 @@ struct BuildState {
     uint32_t *off_cnt, *off_fill, *mg_work;
     uint64_t *off_pos;
     uint32_t mg_warp_bytes;              // shared memory per merging warp
+    uint32_t jt_rows;                    // rows the shared-memory join stages per node (0: join_kernel)
 };
 // Source-node word of a deferred offer: set when the offer is the pair's
 // x <- y insert, whose position decides the source node's `found`.
