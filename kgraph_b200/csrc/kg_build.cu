@@ -413,7 +413,8 @@ __device__ __forceinline__ uint32_t f2ord(float f) {
 }
 __device__ __forceinline__ float ord2f(uint32_t u) { return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u); }
 
-constexpr uint32_t MG_CH = 512;     // offers merged per pass (sorted in shared memory)
+constexpr uint32_t MG_CH = 512;     // offers merged per pass at most (sorted in shared memory)
+constexpr uint32_t MG_PASS = 224;   // offers a value-mode pass aims at
 constexpr int MG_WARPS = 8;
 size_t merge_warp_bytes(uint32_t PS) { return (size_t)MG_CH * 24 + (size_t)PS * 16; }
 
@@ -467,20 +468,98 @@ __global__ void __launch_bounds__(MG_WARPS * 32) offer_merge_kernel(BuildState s
         float rad = s.radius[x];
         bool rad_set = false;
         __syncwarp();
-        for (uint32_t c0 = 0; c0 < m; c0 += MG_CH) {
-            const uint32_t cm = min(MG_CH, m - c0);
+        // The offers go in passes.  Value mode: each pass takes the offers whose
+        // distance key lies in (lo, hi], hi cut from a 32-offer sample so that
+        // about MG_PASS fall in; passes follow in ascending order, so the pass
+        // that meets the first radius rejection ends the pool (every later
+        // offer is farther).  A range that no sample cut keeps within MG_CH
+        // (massive ties) switches the rest of the pool to scan mode: chunks of
+        // up to MG_CH in record order, each merged as it comes.
+        uint32_t lo_key = 0, rem = m, cursor = 0;
+        bool have_lo = false, scan_mode = false, stop = false;
+        while (rem && !stop) {
+            uint32_t cm = 0;
+            if (!scan_mode) {
+                uint32_t hi_key = 0xFFFFFFFFu;
+                int idx = -1;
+                uint32_t sk = 0xFFFFFFFFu;
+                if (rem > MG_PASS) {
+                    const uint32_t si = (uint32_t)(((uint64_t)lane * m) >> 5);
+                    const uint32_t so = f2ord(__uint_as_float(s.off_grp[o0 + si].z));
+                    const bool valid = !have_lo || so > lo_key;
+                    sk = valid ? so : 0xFFFFFFFFu;
+                    for (int kk = 2; kk <= 32; kk <<= 1)   // sort the sample (bitonic across lanes)
+                        for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+                            const uint32_t other = __shfl_xor_sync(FULL, sk, jj);
+                            const bool keep_min = ((lane & jj) == 0) == ((lane & kk) == 0);
+                            sk = keep_min ? min(sk, other) : max(sk, other);
+                        }
+                    const uint32_t nv = __popc(__ballot_sync(FULL, valid));
+                    if (nv == 0) scan_mode = true;
+                    else idx = (int)min(nv - 1, (uint32_t)(((uint64_t)MG_PASS * nv) / rem));
+                }
+                while (!scan_mode) {
+                    if (idx >= 0) hi_key = __shfl_sync(FULL, sk, idx);
+                    cm = 0;
+                    for (uint32_t k0 = 0; k0 < m; k0 += 32) {
+                        const uint32_t k = k0 + lane;
+                        bool in = false;
+                        uint4 o = make_uint4(0u, 0u, 0u, 0u);
+                        uint32_t ko = 0;
+                        if (k < m) {
+                            o = s.off_grp[o0 + k];
+                            ko = f2ord(__uint_as_float(o.z));
+                            in = (!have_lo || ko > lo_key) && ko <= hi_key;
+                        }
+                        const unsigned bal = __ballot_sync(FULL, in);
+                        const uint32_t pos = cm + __popc(bal & ((1u << lane) - 1u));
+                        if (in && pos < MG_CH) {
+                            keys[pos] = ((unsigned long long)ko << 32) | o.y;
+                            vals[pos] = o.w;
+                        }
+                        cm += __popc(bal);
+                    }
+                    if (cm <= MG_CH) {
+                        lo_key = hi_key;
+                        have_lo = true;
+                        break;
+                    }
+                    if (idx <= 0) scan_mode = true;   // ties: no cut fits one pass
+                    else idx /= 2;
+                }
+                __syncwarp();
+            }
+            if (scan_mode) {   // the next chunk of the remaining offers in record order
+                cm = 0;
+                while (cursor < m && cm < MG_CH) {
+                    const uint32_t k = cursor + lane;
+                    bool in = false;
+                    uint4 o = make_uint4(0u, 0u, 0u, 0u);
+                    uint32_t ko = 0;
+                    if (k < m) {
+                        o = s.off_grp[o0 + k];
+                        ko = f2ord(__uint_as_float(o.z));
+                        in = !have_lo || ko > lo_key;
+                    }
+                    const unsigned bal = __ballot_sync(FULL, in);
+                    const uint32_t take = min((uint32_t)__popc(bal), MG_CH - cm);
+                    const uint32_t rank = __popc(bal & ((1u << lane) - 1u));
+                    if (in && rank < take) {
+                        keys[cm + rank] = ((unsigned long long)ko << 32) | o.y;
+                        vals[cm + rank] = o.w;
+                    }
+                    cursor += (take < (uint32_t)__popc(bal)) ? (uint32_t)(__fns(bal, 0, take + 1)) : 32u;
+                    cm += take;
+                }
+                __syncwarp();
+            }
+            if (cm == 0) break;   // nothing left (the counts agree; this only guards the loop)
+            rem -= cm;
             uint32_t P2 = 32;
             while (P2 < cm) P2 <<= 1;
-            for (uint32_t k = lane; k < P2; k += 32) {
-                unsigned long long key = ~0ull;
-                uint32_t v = 0;
-                if (k < cm) {
-                    const uint4 o = s.off_grp[o0 + c0 + k];
-                    key = ((unsigned long long)f2ord(__uint_as_float(o.z)) << 32) | o.y;
-                    v = o.w;
-                }
-                keys[k] = key;
-                vals[k] = v;
+            for (uint32_t k = cm + lane; k < P2; k += 32) {
+                keys[k] = ~0ull;
+                vals[k] = 0;
             }
             __syncwarp();
             for (uint32_t kk = 2; kk <= P2; kk <<= 1) {   // bitonic sort, ascending (distance, id)
@@ -562,6 +641,7 @@ __global__ void __launch_bounds__(MG_WARPS * 32) offer_merge_kernel(BuildState s
             __syncwarp();
             const bool full_main = qs + Lc > L;   // an insert reached a full list
             uint32_t ntail = 0;
+            bool rejected = false;
             if (Lc + qs >= L && lane == 0) {
                 // the offers beyond the list, in order (lane 0; a short run: at most one offer
                 // above the list's last distance can land)
@@ -576,7 +656,7 @@ __global__ void __launch_bounds__(MG_WARPS * 32) offer_merge_kernel(BuildState s
                 for (uint32_t k = lo; k < cm; ++k) {
                     if (paux[k] < L) continue;
                     const float d = ord2f((uint32_t)(keys[k] >> 32));
-                    if (d > rc) break;
+                    if (d > rc) { rejected = true; break; }
                     const uint32_t c = (uint32_t)keys[k];
                     bool dup = false;
                     for (int j = (int)L - 1; !dup && j >= 0 && pdn[j] == d; --j) dup = (pin[j] & ID_MASK) == c;
@@ -588,6 +668,8 @@ __global__ void __launch_bounds__(MG_WARPS * 32) offer_merge_kernel(BuildState s
                 }
             }
             ntail = __shfl_sync(FULL, ntail, 0);
+            // a radius rejection in value mode: the offers still to come are all farther
+            stop = !scan_mode && __shfl_sync(FULL, rejected, 0);
             __syncwarp();
             // counts: offers that passed the radius test (duplicates included), and those that landed
             att += (cm - nnd) + qs + ntail;

@@ -159,3 +159,15 @@ def test_deferred_and_locked_builds_agree(gpu_ctx):
     # the deferred build counts its merged offers: attempts >= landed > 0
     it = out["deferred"][2]
     assert sum(r["insert_attempts"] for r in it) >= sum(r["inserts_landed"] for r in it) > 0
+
+
+def test_merge_of_many_offers_equals_serial_inserts(gpu_ctx):
+    """Pools with up to 3,000 offers and well-spread distances: the merge takes
+    them in ascending distance ranges (several passes, the last one ending at
+    the first radius rejection), which is the serial ascending order itself."""
+    L, K = 100, 50
+    case = _case(6, 16, L, 3000, ids=5000, dmax=1_000_000)
+    got = gpu_ctx.join_merge_check(L, K, *case)
+    ref = _serial(case, L, K)
+    for name, g, r in zip(("pool distances", "pool ids", "L", "radius", "found"), got, ref):
+        assert np.array_equal(np.asarray(g).view(np.uint32), np.asarray(r).view(np.uint32)), name
