@@ -322,6 +322,37 @@ __global__ void __launch_bounds__(256) join_kernel(BuildState s) {
 // rows cross from L2/DRAM once per node instead of once per pair.  Pairs: for
 // new entry i (warp-strided), new[i+1 ..) then old, as join_kernel.
 constexpr int JT_WARPS = 4;
+constexpr uint32_t JT_BUF = 64;   // offers a warp collects before it appends them to the record buffer
+// Shared memory of join_tile_kernel besides the rows: per list entry its id,
+// norm term and radius, per warp the offer buffer.
+__host__ __device__ constexpr size_t jt_fixed_bytes(uint32_t list_cap) {
+    return (size_t)list_cap * 12 + (size_t)JT_WARPS * JT_BUF * 16;
+}
+
+// Deferred mode: the offers a warp collected (all of the CTA's current node)
+// go to the record buffer with one cursor atomic; those beyond its capacity
+// are inserted under the lock here (their uu counts for the current node).
+__device__ __forceinline__ void jt_flush(const BuildState &s, uint4 *buf, uint32_t &cnt, int lane, bool &uu,
+                                         InsertTally &tally) {
+    if (!cnt) return;
+    unsigned long long b0 = 0;
+    if (lane == 0) b0 = atomicAdd(s.off_cursor, (unsigned long long)cnt);
+    b0 = __shfl_sync(FULL, b0, 0);
+    const uint32_t fit = b0 >= s.off_cap ? 0u : (uint32_t)min((unsigned long long)cnt, s.off_cap - b0);
+    for (uint32_t k = lane; k < fit; k += 32) {
+        const uint4 o = buf[k];
+        s.off_lin[b0 + k] = o;
+        atomicAdd(s.off_cnt + o.x, 1u);
+    }
+    for (uint32_t k = fit; k < cnt; ++k) {
+        const uint4 o = buf[k];
+        const uint32_t r = locked_insert(s, o.x, o.y, __uint_as_float(o.z), lane, tally);
+        if ((o.w & OFFER_UU) && r < s.K) uu = true;
+    }
+    cnt = 0;
+    __syncwarp();
+}
+
 __global__ void __launch_bounds__(JT_WARPS * 32) join_tile_kernel(BuildState s) {
     extern __shared__ __align__(16) float jt_smem[];
     __shared__ uint32_t s_node, s_uu;
@@ -329,11 +360,17 @@ __global__ void __launch_bounds__(JT_WARPS * 32) join_tile_kernel(BuildState s) 
     const int g = lane >> 2, t = lane & 3;
     const uint32_t N = s.D.n, stride = s.D.ld + 4;   // 16 bytes of padding: rows start on different banks
     const int metric = s.D.metric;
-    float *rows = jt_smem;
+    const uint32_t cap = s.NEWCAP + s.OLDCAP;
+    uint4 *bufs = reinterpret_cast<uint4 *>(jt_smem);   // 16-byte aligned at the start
+    uint4 *buf = bufs + (size_t)warp * JT_BUF;
+    float *rows = reinterpret_cast<float *>(bufs + (size_t)JT_WARPS * JT_BUF);
     float *nrm = rows + (size_t)s.jt_rows * stride;
-    uint32_t *uid = reinterpret_cast<uint32_t *>(nrm + s.NEWCAP + s.OLDCAP);
+    float *rad = nrm + cap;
+    uint32_t *uid = reinterpret_cast<uint32_t *>(rad + cap);
+    const bool deferred = s.off_lin != nullptr;
     unsigned long long comps = 0;
     InsertTally tally;
+    uint32_t bcnt = 0;
     for (;;) {
         if (threadIdx.x == 0) { s_node = atomicAdd(s.work, 1u); s_uu = 0; }
         __syncthreads();
@@ -352,6 +389,9 @@ __global__ void __launch_bounds__(JT_WARPS * 32) join_tile_kernel(BuildState s) 
             if (id >= N) { raise_error(s.err, ERR_BAD_ID); id = NO_ID; }
             uid[u] = id;
             nrm[u] = (id != NO_ID && metric != METRIC_L2SQR) ? s.D.norms[id] : 0.f;
+            // deferred: the radii as the join starts (they change only in the merge after it; a
+            // larger radius lets more offers through to the merge's exact test)
+            rad[u] = id != NO_ID ? *reinterpret_cast<volatile float *>(s.radius + id) : 0.f;
         }
         __syncthreads();
         const uint32_t staged = min(U, s.jt_rows);
@@ -366,7 +406,7 @@ __global__ void __launch_bounds__(JT_WARPS * 32) join_tile_kernel(BuildState s) 
         for (uint32_t i = warp; i < a; i += JT_WARPS) {
             const uint32_t idi = uid[i];
             const float *ri = i < s.jt_rows ? rows + (size_t)i * stride : s.D.X + (size_t)(idi == NO_ID ? 0u : idi) * s.D.ld;
-            const float ni = nrm[i];
+            const float ni = nrm[i], radi = rad[i];
             const uint32_t nnn = a - 1 - i, inner = nnn + b;   // partners: new[i+1..a) then old
             for (uint32_t base = 0; base < inner; base += 8) {
                 const uint32_t k = base + g;
@@ -379,10 +419,28 @@ __global__ void __launch_bounds__(JT_WARPS * 32) join_tile_kernel(BuildState s) 
                 const float *rj = u < s.jt_rows ? rows + (size_t)u * stride : s.D.X + (size_t)(jid == NO_ID ? 0u : jid) * s.D.ld;
                 const float raw = group4_raw(ri, rj, (int)s.D.d, metric, t, FULL);
                 const float dd = metric == METRIC_L2SQR ? raw : finish_metric(raw, ni, nrm[u], metric);
-                settle_pass(s, lane, t, v, v ? (is_nn ? min(idi, jid) : idi) : 0u, v ? (is_nn ? max(idi, jid) : jid) : 0u,
-                            dd, n, comps, uu, tally);
+                const bool i_is_x = !is_nn || idi < jid;
+                const uint32_t x = v ? (i_is_x ? idi : jid) : 0u, y = v ? (i_is_x ? jid : idi) : 0u;
+                if (!deferred) {
+                    settle_pass(s, lane, t, v, x, y, dd, n, comps, uu, tally);
+                    continue;
+                }
+                // the unlocked radius test of both directions (kgraph.cpp:725) on the staged radii
+                const float rx = i_is_x ? radi : rad[u], ry = i_is_x ? rad[u] : radi;
+                comps += __popc(__ballot_sync(FULL, v && t == 0));
+                const bool off = v && ((t == 0 && !(dd > rx)) || (t == 1 && !(dd > ry)));
+                const unsigned om = __ballot_sync(FULL, off);
+                if (!om) continue;
+                if (bcnt + __popc(om) > JT_BUF) jt_flush(s, buf, bcnt, lane, uu, tally);
+                if (off) {
+                    const uint32_t pos = bcnt + __popc(om & ((1u << lane) - 1u));
+                    buf[pos] = make_uint4(t == 0 ? x : y, t == 0 ? y : x, __float_as_uint(dd), n | (t == 0 ? OFFER_UU : 0u));
+                }
+                bcnt += __popc(om);
+                __syncwarp();
             }
         }
+        if (deferred) jt_flush(s, buf, bcnt, lane, uu, tally);
         if (uu && lane == 0) atomicOr(&s_uu, 1u);
         __syncthreads();
         if (threadIdx.x == 0) s.found[n] = s_uu;
@@ -1111,7 +1169,7 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
     int jt_blocks = 0;
     s.jt_rows = 0;
     if (ctx->join_tile) {
-        const size_t fixed = (size_t)(s.NEWCAP + s.OLDCAP) * 8;
+        const size_t fixed = jt_fixed_bytes(s.NEWCAP + s.OLDCAP);
         const size_t row_bytes = (size_t)(s.D.ld + 4) * 4;
         const size_t budget = 48 * 1024 - 64;
         if (budget > fixed + 8 * row_bytes) {
