@@ -1168,7 +1168,9 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
     size_t jt_smem = 0;
     int jt_blocks = 0;
     s.jt_rows = 0;
-    if (ctx->join_tile) {
+    // (with locked inserts the warp-per-node join: four warps of one node contend for the
+    // same pools' locks)
+    if (ctx->join_tile && ctx->join_inserts != KG_INSERTS_LOCKED) {
         const size_t fixed = jt_fixed_bytes(s.NEWCAP + s.OLDCAP);
         const size_t row_bytes = (size_t)(s.D.ld + 4) * 4;
         const size_t budget = 48 * 1024 - 64;
@@ -1211,6 +1213,7 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
                 return cuda_fail(ctx, e, "join merge");
         }
     }
+    if (!s.off_lin) s.jt_rows = 0;   // locked inserts: the warp-per-node join
 
     // GenerateControl (kgraph.cpp:254-270): C distinct random nodes, exact K-NN.
     if (g_verbosity > 0) std::cerr << "Generating control..." << std::endl;
