@@ -49,10 +49,11 @@ TARGET = 0.95
 # DRAM read + write from one-pass ncu captures (dram__bytes_read.sum +
 # dram__bytes_write.sum) of this workload at full size (1M x 128, 10,000
 # queries, K=10), per launch: the plain walk at P=1000, the router-seeded walk
-# at P=5, and the local join summed over the 30 join launches of one warm build.
-SEARCH_DRAM_BYTES_PER_LAUNCH = 114.45e9
-ROUTER_SEARCH_DRAM_BYTES_PER_LAUNCH = 18.00e9
-BUILD_JOIN_DRAM_BYTES = 2124.3e9
+# at P=5, and the local join (the shared-memory join, the offers' scatter and
+# the pools' merge) summed over the iterations of one warm build.
+SEARCH_DRAM_BYTES_PER_LAUNCH = 136.02e9
+ROUTER_SEARCH_DRAM_BYTES_PER_LAUNCH = 17.35e9
+BUILD_JOIN_DRAM_BYTES = 364.7e9
 
 
 def _sample(c, n, rng, d):
@@ -872,8 +873,9 @@ def main():
                                        "achieved": build_bytes / (build_ms / 1000) / 1e9, "peak": hbm,
                                        "unit": "GB/s", "frac": build_bytes / (build_ms / 1000) / 1e9 / hbm,
                                        "peak_source": peak_source, "traffic": BUILD_JOIN_DRAM_BYTES,
-                                       "traffic_note": "join_kernel launches of one build; each node's partner "
-                                                       "rows are read once per two of its new entries",
+                                       "traffic_note": "join_tile_kernel + offer_scatter_kernel + offer_merge_kernel "
+                                                       "launches of one build; each node's rows are read once into "
+                                                       "shared memory",
                                        "bytes": "join list entries x (4 D + 4) + iterations run x N x 2 (L+1) x 12"}},
                 "build_parity": parity,
                 # per step: the queries in, and the ids buffer in (the library keeps a caller's entries
