@@ -352,19 +352,29 @@ int kg_set_join_precision(kg_ctx *ctx, int mode);
  *                        inserts that the reference's threads can produce, with
  *                        the same duplicate, radius, L and `found` rules; offers
  *                        beyond the record buffer's capacity (sized from free
- *                        device memory, at most 20 GB) are inserted under the
- *                        lock during the join;
+ *                        device memory, at most 20 GB; a join that needs more
+ *                        runs in rounds of consecutive nodes) are inserted under
+ *                        the lock during the join;
  *   KG_INSERTS_AUTO      (default) KG_INSERTS_DEFERRED.
  * The tensor-core joins (KG_JOIN_BF16 / KG_JOIN_FP8 iterations) always lock. */
 enum { KG_INSERTS_AUTO = 0, KG_INSERTS_LOCKED = 1, KG_INSERTS_DEFERRED = 2 };
 int kg_set_join_inserts(kg_ctx *ctx, int mode);
+/* Bound on the deferred inserts' record buffers, in offers (32 bytes of device
+ * memory each; 0 = automatic: 30 % of free memory, at most 20 GB).  A join
+ * whose first-iteration offers (at most 2 x C(2S, 2) per node) exceed it runs
+ * in rounds of consecutive nodes, each with its own merge; offers beyond it
+ * within a round are inserted under the lock.  No counterpart in the
+ * reference. */
+int kg_set_join_offer_capacity(kg_ctx *ctx, size_t offers);
 /* Check entry point of the deferred inserts' merge, on caller data: n pools of
  * L+1 entries (rows of L+1: distances, ids with the new-flag in bit 31), their
  * list lengths and radii (updated in place), and n_off offers (target pool,
  * candidate id, distance, source node with bit 31 set for a pair's x <- y
  * offer); found[source] is set to 1 where such an offer lands below K (other
  * entries 0).  A pool's offers are merged in ascending (distance, id) order in
- * passes of at most 512.  No counterpart in the reference. */
+ * passes of at most 512; `found` follows the serial inserts in the caller's
+ * order of each pool's offers (their arrival order).  No counterpart in the
+ * reference. */
 int kg_join_merge_check(kg_ctx *ctx, unsigned n, unsigned L, unsigned K, float *pool_d, uint32_t *pool_i,
                         uint32_t *nodeL, float *radius, size_t n_off, const uint32_t *target, const uint32_t *cand,
                         const float *dist, const uint32_t *src, uint32_t *found);

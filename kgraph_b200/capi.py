@@ -21,7 +21,7 @@ SYMBOLS = [
     "kg_graph_export", "kg_graph_import", "kg_search_batch", "kg_reverse", "kg_prune", "kg_last_timing",
     "kg_last_search_work", "kg_search_batch_noalloc", "kg_noalloc_scratch_bytes",
     "kg_router_params_default", "kg_router_train", "kg_router_seeds", "kg_router_gradients", "kg_last_router_timing",
-    "kg_set_join_precision", "kg_set_join_inserts", "kg_join_merge_check", "kg_last_join_stats", "kg_last_build_graphs", "kg_search_autotune",
+    "kg_set_join_precision", "kg_set_join_inserts", "kg_set_join_offer_capacity", "kg_join_merge_check", "kg_last_join_stats", "kg_last_build_graphs", "kg_search_autotune",
     "kg_set_search_tuning", "kg_get_search_tuning", "kg_last_search_shape", "kg_set_search_precision",
     "kg_last_search_filter",
     "kg_filter_bounds", "kg_router_search", "kg_tc_gemm_check", "kg_tc_assign_check", "kg_last_build_work",
@@ -131,6 +131,7 @@ def lib():
                                           C.POINTER(C.c_float), vp]
         L.kg_set_join_precision.argtypes = [vp, C.c_int]
         L.kg_set_join_inserts.argtypes = [vp, C.c_int]
+        L.kg_set_join_offer_capacity.argtypes = [vp, sz]
         L.kg_join_merge_check.argtypes = [vp, C.c_uint, C.c_uint, C.c_uint, vp, vp, vp, vp, sz, vp, vp, vp, vp, vp]
         L.kg_last_join_stats.argtypes = [vp, C.POINTER(JoinStats)]
         L.kg_last_build_graphs.argtypes = [vp, C.POINTER(C.c_uint)]
@@ -403,6 +404,10 @@ class Context:
         self._check(self.L.kg_join_merge_check(self.h, n, L, K, _ptr(pd), _ptr(pi), _ptr(nl), _ptr(rd), len(t),
                                                _ptr(t), _ptr(c), _ptr(d), _ptr(s_), _ptr(found)))
         return pd, pi, nl, rd, found
+
+    def set_join_offer_capacity(self, offers):
+        """kg_set_join_offer_capacity: bound the deferred inserts' record buffers (0 = automatic)."""
+        self._check(self.L.kg_set_join_offer_capacity(self.h, int(offers)))
 
     def set_join_inserts(self, mode):
         """kg_set_join_inserts: 'auto', 'locked' or 'deferred'."""

@@ -205,57 +205,6 @@ __device__ __forceinline__ void pair_dist_shared(const DataView &D, uint32_t j, 
 }
 
 // ------------------------------------------------------------------ join
-// One pass of 8 pairs (one per 4-lane group: lanes 4p..4p+3 hold pair p's
-// x, y and distance, valid marking a pair to evaluate; node n's join made
-// them): the unlocked radius pre-test for both directions (kgraph.cpp:725),
-// then Nhood::parallel_try_insert of the offers that passed -- recorded for
-// the deferred merge while the record buffer has room, else under the
-// target's lock here.  uu is set when an x <- y insert lands below K
-// (kgraph.cpp:808-810); comps counts the pairs (the reference's cc).
-__device__ __forceinline__ void settle_pass(const BuildState &s, int lane, int t, bool valid, uint32_t x, uint32_t y,
-                                            float dd, uint32_t n, unsigned long long &comps, bool &uu,
-                                            InsertTally &tally) {
-    const float rx = (valid && t == 0) ? *reinterpret_cast<volatile float *>(s.radius + x) : 0.f;
-    const float ry = (valid && t == 1) ? *reinterpret_cast<volatile float *>(s.radius + y) : 0.f;
-    const unsigned vm_all = __ballot_sync(FULL, valid && t == 0);
-    unsigned nx = __ballot_sync(FULL, valid && t == 0 && !(dd > rx));
-    unsigned ny = __ballot_sync(FULL, valid && t == 1 && !(dd > ry));
-    comps += __popc(vm_all);
-    if (s.off_lin && (nx | ny)) {
-        // deferred: the offers go to the grouped merge after the join (one
-        // cursor atomic per pass); those beyond the buffer's capacity are
-        // inserted here under the lock
-        const unsigned om = nx | ny;
-        unsigned long long b0 = 0;
-        if (lane == 0) b0 = atomicAdd(s.off_cursor, (unsigned long long)__popc(om));
-        b0 = __shfl_sync(FULL, b0, 0);
-        const unsigned long long fit = b0 >= s.off_cap ? 0ull : s.off_cap - b0;
-        const uint32_t rank = __popc(om & ((1u << lane) - 1u));
-        const bool mine = ((om >> lane) & 1u) && rank < fit;
-        if (mine) {
-            const uint32_t tg = t == 0 ? x : y;
-            s.off_lin[b0 + rank] = make_uint4(tg, t == 0 ? y : x, __float_as_uint(dd), n | (t == 0 ? OFFER_UU : 0u));
-            atomicAdd(s.off_cnt + tg, 1u);
-        }
-        const unsigned dm = __ballot_sync(FULL, mine);
-        nx &= ~dm;
-        ny &= ~dm;
-    }
-    // only the pairs with an offer that passed a radius test: a pair both endpoints reject
-    // inserts nothing and leaves r at pool.size() (>= K)
-    unsigned vm = nx | (ny >> 1);
-    while (vm) {
-        const int src = __ffs(vm) - 1;
-        vm &= vm - 1;
-        const uint32_t xg = __shfl_sync(FULL, x, src), yg = __shfl_sync(FULL, y, src);
-        const float dg = __shfl_sync(FULL, dd, src);
-        uint32_t r = s.Lp;
-        if (nx & (1u << src)) r = locked_insert(s, xg, yg, dg, lane, tally);
-        if (r < s.K) uu = true;
-        if (ny & (1u << (src + 1))) locked_insert(s, yg, xg, dg, lane, tally);
-    }
-}
-
 // KGraphConstructor::join + Nhood::join (kgraph.cpp:740-751, 797-815).  The
 // node's new entries are taken two at a time: the second one's partners are
 // the first one's minus the second itself, so each partner row read serves
@@ -268,9 +217,9 @@ __global__ void __launch_bounds__(256) join_kernel(BuildState s) {
     InsertTally tally;
     for (;;) {
         uint32_t n = 0;
-        if (lane == 0) n = atomicAdd(s.work, 1u);
+        if (lane == 0) n = s.node_lo + atomicAdd(s.work, 1u);
         n = __shfl_sync(FULL, n, 0);
-        if (n >= N) break;
+        if (n >= s.node_hi) break;
         const uint32_t a = s.cnt_new[n], b = s.cnt_old[n];
         const uint32_t *nw = s.nn_new + (size_t)n * s.NEWCAP;
         const uint32_t *od = s.nn_old + (size_t)n * s.OLDCAP;
@@ -372,10 +321,10 @@ __global__ void __launch_bounds__(JT_WARPS * 32) join_tile_kernel(BuildState s) 
     InsertTally tally;
     uint32_t bcnt = 0;
     for (;;) {
-        if (threadIdx.x == 0) { s_node = atomicAdd(s.work, 1u); s_uu = 0; }
+        if (threadIdx.x == 0) { s_node = s.node_lo + atomicAdd(s.work, 1u); s_uu = 0; }
         __syncthreads();
         const uint32_t n = s_node;
-        if (n >= N) break;
+        if (n >= s.node_hi) break;
         const uint32_t a = min(s.cnt_new[n], s.NEWCAP), b = min(s.cnt_old[n], s.OLDCAP);
         if (a == 0) {
             if (threadIdx.x == 0) s.found[n] = 0u;
@@ -526,6 +475,76 @@ __global__ void __launch_bounds__(MG_WARPS * 32) offer_merge_kernel(BuildState s
         float rad = s.radius[x];
         bool rad_set = false;
         __syncwarp();
+        // `found` (kgraph.cpp:808-810): an x <- y insert that lands below K at its
+        // time.  Whether an insert lands below K depends on the order the offers
+        // arrive in, not only on the final list; the reference's threads deliver
+        // them in an arbitrary interleaving, and so does the grouping here (record
+        // order within a pool), so the offers are replayed in that order against a
+        // copy of the list's first K positions -- the positions below K are all
+        // that decide it, an entry pushed past them never comes back, and a
+        // duplicate of an entry pushed past them lands at K or later anyway; a
+        // duplicate's return value (the list's length + 1) is below K only while
+        // the copy holds the whole list.
+        {
+            const uint32_t Kc = min(s.K, L);
+            float *kd = pdn;
+            uint32_t *ki = pin;
+            uint32_t kc = min(Lc, Kc);
+            for (uint32_t j = lane; j < kc; j += 32) { kd[j] = pd[j]; ki[j] = pi[j]; }
+            __syncwarp();
+            float kth = kc == Kc && Kc ? kd[Kc - 1] : FLT_MAX;
+            // 32 offers at a time, in arrival order.  An offer lands below K iff (the
+            // copy's entries <= d) + (earlier non-duplicate offers of its chunk with
+            // distance <= d) < K: an earlier offer that does not land is no closer
+            // than one that does, so counting it never changes the answer.
+            for (uint32_t k0 = 0; k0 < m && Kc; k0 += 32) {
+                const uint32_t k = k0 + lane;
+                uint4 o = make_uint4(0u, 0u, 0u, 0u);
+                if (k < m) o = s.off_grp[o0 + k];
+                const float d = __uint_as_float(o.z);
+                const bool possible = k < m && (kc < Kc || d < kth);
+                if (!__any_sync(FULL, possible)) continue;
+                uint32_t base = 0;
+                bool dupK = false;
+                if (possible) {
+                    uint32_t lo = 0, hi = kc;   // the copy's entries <= d
+                    while (lo < hi) {
+                        const uint32_t mid = (lo + hi) >> 1;
+                        if (kd[mid] <= d) lo = mid + 1; else hi = mid;
+                    }
+                    base = lo;
+                    for (int j = (int)base - 1; !dupK && j >= 0 && kd[j] == d; --j) dupK = (ki[j] & ID_MASK) == o.y;
+                }
+                // the first of identical offers (same distance and id) in the chunk
+                const unsigned long long key = possible ? (((unsigned long long)o.z << 32) | o.y) : ~0ull - lane;
+                const unsigned same = __match_any_sync(FULL, key);
+                const int first = __ffs(same) - 1;
+                const bool nd = possible && !dupK && first == lane;
+                const unsigned ndm = __ballot_sync(FULL, nd);
+                uint32_t cnt = 0;
+                for (unsigned rest = ndm; rest; rest &= rest - 1) {   // ndm is warp-uniform
+                    const int j = __ffs(rest) - 1;
+                    const float dj = __shfl_sync(FULL, d, j);
+                    if (j < lane && dj <= d) ++cnt;
+                }
+                const bool landed = nd && base + cnt < Kc;
+                const unsigned lm = __ballot_sync(FULL, landed);
+                const bool first_landed = (lm >> first) & 1u;
+                if (landed && (o.w & OFFER_UU)) s.found[o.w & ~OFFER_UU] = 1u;
+                // a duplicate returns the list's length + 1 (kgraph.cpp:193): below K only while
+                // the copy holds the whole list
+                const bool dup = possible && (dupK || (first != lane && first_landed));
+                if (dup && (o.w & OFFER_UU) && kc + __popc(lm & ((1u << lane) - 1u)) + 1 < s.K)
+                    s.found[o.w & ~OFFER_UU] = 1u;
+                if (lm) {
+                    uint32_t mr;
+                    kc = warp_batch_insert(kd, ki, nullptr, kc, Kc + 1, lm, d, o.y | FLAG_BIT, 0u, &mr, lane);
+                    __syncwarp();
+                    kth = kc == Kc ? kd[Kc - 1] : FLT_MAX;
+                }
+            }
+            __syncwarp();
+        }
         // The offers go in passes.  Value mode: each pass takes the offers whose
         // distance key lies in (lo, hi], hi cut from a 32-offer sample so that
         // about MG_PASS fall in; passes follow in ascending order, so the pass
@@ -674,8 +693,6 @@ __global__ void __launch_bounds__(MG_WARPS * 32) offer_merge_kernel(BuildState s
                 if (p < L) {
                     ++qs;
                     acc_d[qaux[k]] = ord2f((uint32_t)(keys[k] >> 32));
-                    const uint32_t v = vals[k];
-                    if ((v & OFFER_UU) && p < s.K) s.found[v & ~OFFER_UU] = 1u;
                 }
             }
             for (int o = 16; o; o >>= 1) qs += __shfl_xor_sync(FULL, qs, o);
@@ -1103,6 +1120,8 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
     BuildState s{};
     s.D = DataView{ctx->X.as<float>(), ctx->norms.as<float>(), N, ctx->d, ctx->ld, ctx->metric};
     s.L = L; s.Lp = L + 1; s.K = K; s.S = S; s.R = params->R;
+    s.node_lo = 0;
+    s.node_hi = N;
     s.PS = (s.Lp + 7) / 8 * 8;
     s.NEWCAP = std::max(2 * S, L) + s.R;
     s.OLDCAP = L + s.R;
@@ -1192,7 +1211,8 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
         const size_t own = ctx->offer_lin.bytes + ctx->offer_grp.bytes;
         size_t cap = std::min<size_t>((size_t)20 << 30, (freeb + own) / 10 * 3) / 32;
         cap = std::min<size_t>(cap, n * 1024);
-        if (cap >= 1024) {
+        if (ctx->offer_cap) cap = std::min(cap, std::max<size_t>(ctx->offer_cap, 64));
+        if (cap >= 1024 || (ctx->offer_cap && cap >= 64)) {
             if ((e = ctx->offer_lin.reserve(cap * 16)) != cudaSuccess || (e = ctx->offer_grp.reserve(cap * 16)) != cudaSuccess ||
                 (e = ctx->offer_aux.reserve((n + 1) * 8 + (n + 1) * 4 + n * 4 + 16)) != cudaSuccess)
                 return cuda_fail(ctx, e, "alloc join offers");
@@ -1272,24 +1292,44 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
 
     // One iteration's device work, recorded into the stream: the FP32 join,
     // the statistics with their copies to the host, and the update.
+    // A deferred join goes in rounds of consecutive nodes (join, grouping and
+    // merge each), as many as keep a round's offers -- at most 2 x C(2S, 2)
+    // per node in the first iteration -- within the record buffer; any order
+    // of rounds is a serial order of the same inserts.
+    const uint32_t join_rounds =
+        s.off_lin ? (uint32_t)std::min<uint64_t>(64, std::max<uint64_t>(1, ((uint64_t)N * 2 * S * (2 * S - 1) + s.off_cap - 1) / s.off_cap))
+                  : 1u;
+    // The deferred inserts around one join round: the record cursor and counts
+    // cleared before it; the grouping and the pools' merge after it.
+    auto rec_offers_begin = [&]() {
+        cudaMemsetAsync(s.off_cursor, 0, 16, st);   // the offer cursor and the merge's claim counter
+        cudaMemsetAsync(s.off_cnt, 0, (n + 1) * 4, st);
+        cudaMemsetAsync(s.off_fill, 0, n * 4, st);
+    };
+    auto rec_offers_end = [&](const BuildState &sr) -> cudaError_t {
+        size_t sb = offer_scan_bytes;
+        cudaError_t e2 = cub::DeviceScan::ExclusiveSum(ctx->offer_scan.p, sb, s.off_cnt, s.off_pos, N + 1, st);
+        if (e2 != cudaSuccess) return e2;
+        offer_scatter_kernel<<<grid_for(ctx), 256, 0, st>>>(sr);
+        const int bps = std::max(1, (int)((228u << 10) / ((size_t)mg_warps * s.mg_warp_bytes + 1024)));
+        offer_merge_kernel<<<ctx->num_sms * bps, mg_warps * 32, (size_t)mg_warps * s.mg_warp_bytes, st>>>(sr);
+        return cudaGetLastError();
+    };
     auto rec_join = [&]() -> cudaError_t {
-        cudaMemsetAsync(s.work, 0, 4, st);
-        if (s.off_lin) {
-            cudaMemsetAsync(s.off_cursor, 0, 16, st);   // the offer cursor and the merge's claim counter
-            cudaMemsetAsync(s.off_cnt, 0, (n + 1) * 4, st);
-            cudaMemsetAsync(s.off_fill, 0, n * 4, st);
-        }
-        if (s.jt_rows)
-            join_tile_kernel<<<ctx->num_sms * jt_blocks, JT_WARPS * 32, jt_smem, st>>>(s);
-        else
-            join_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
-        if (s.off_lin) {
-            size_t sb = offer_scan_bytes;
-            cudaError_t e2 = cub::DeviceScan::ExclusiveSum(ctx->offer_scan.p, sb, s.off_cnt, s.off_pos, N + 1, st);
-            if (e2 != cudaSuccess) return e2;
-            offer_scatter_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
-            const int bps = std::max(1, (int)((228u << 10) / ((size_t)mg_warps * s.mg_warp_bytes + 1024)));
-            offer_merge_kernel<<<ctx->num_sms * bps, mg_warps * 32, (size_t)mg_warps * s.mg_warp_bytes, st>>>(s);
+        for (uint32_t r = 0; r < join_rounds; ++r) {
+            BuildState sr = s;
+            sr.node_lo = (uint32_t)((uint64_t)N * r / join_rounds);
+            sr.node_hi = (uint32_t)((uint64_t)N * (r + 1) / join_rounds);
+            cudaMemsetAsync(s.work, 0, 4, st);
+            if (s.off_lin) rec_offers_begin();
+            if (s.jt_rows)
+                join_tile_kernel<<<ctx->num_sms * jt_blocks, JT_WARPS * 32, jt_smem, st>>>(sr);
+            else
+                join_kernel<<<grid_for(ctx), 256, 0, st>>>(sr);
+            if (s.off_lin) {
+                cudaError_t e2 = rec_offers_end(sr);
+                if (e2 != cudaSuccess) return e2;
+            }
         }
         return cudaGetLastError();
     };
@@ -1365,9 +1405,12 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
             if ((e = ctx->joinb.reserve((size_t)(R + 1) * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc");
             jq.bounds = ctx->joinb.as<uint32_t>();
             if ((e = join_tc_bounds(st, jpre, N, slab, R, jq.bounds)) != cudaSuccess) return cuda_fail(ctx, e, "join");
-            for (uint32_t r = 0; r < R; ++r)
+            for (uint32_t r = 0; r < R; ++r) {
+                if (s.off_lin) rec_offers_begin();
                 if ((e = launch_join_tc(ctx->num_sms, grid_for(ctx), st, s, jq, r, fp8 ? 1 : 0)) != cudaSuccess)
                     return cuda_fail(ctx, e, "join");
+                if (s.off_lin && (e = rec_offers_end(s)) != cudaSuccess) return cuda_fail(ctx, e, "join merge");
+            }
             if ((e = run_graph(g_stats, rec_stats)) != cudaSuccess) return cuda_fail(ctx, e, "statistics graph");
         } else if (pending_update) {
             e = run_graph(g_steady, [&]() -> cudaError_t {
@@ -1566,12 +1609,19 @@ extern "C" int kg_join_merge_check(kg_ctx *ctx, unsigned n, unsigned L, unsigned
     std::vector<uint32_t> hi((size_t)n * s.PS, UNSET_ID), cnt(n + 1, 0);
     for (size_t x = 0; x < n; ++x)
         for (uint32_t j = 0; j < s.Lp; ++j) { hd[x * s.PS + j] = pool_d[x * s.Lp + j]; hi[x * s.PS + j] = pool_i[x * s.Lp + j]; }
+    // grouped by target on the host, each pool's offers in the caller's order (the order they
+    // arrive in for the merge's `found` replay)
     std::vector<uint4> lin(std::max<size_t>(n_off, 1));
-    for (size_t k = 0; k < n_off; ++k) {
-        uint32_t db;
-        std::memcpy(&db, &dist[k], 4);
-        lin[k] = make_uint4(target[k], cand[k], db, src[k]);
-        ++cnt[target[k]];
+    std::vector<uint64_t> pos(n + 1, 0);
+    for (size_t k = 0; k < n_off; ++k) ++cnt[target[k]];
+    for (size_t x = 0; x < n; ++x) pos[x + 1] = pos[x] + cnt[x];
+    {
+        std::vector<uint64_t> fill(pos.begin(), pos.end() - 1);
+        for (size_t k = 0; k < n_off; ++k) {
+            uint32_t db;
+            std::memcpy(&db, &dist[k], 4);
+            lin[fill[target[k]]++] = make_uint4(target[k], cand[k], db, src[k]);
+        }
     }
     DevBuf b[10];
     cudaError_t e;
@@ -1601,13 +1651,10 @@ extern "C" int kg_join_merge_check(kg_ctx *ctx, unsigned n, unsigned L, unsigned
     cudaMemcpyAsync(s.nodeL, nodeL, (size_t)n * 4, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(s.radius, radius, (size_t)n * 4, cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(s.found, 0, (size_t)n * 4, st);
-    cudaMemcpyAsync(s.off_lin, lin.data(), lin.size() * 16, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(s.off_grp, lin.data(), lin.size() * 16, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(s.off_cnt, cnt.data(), (size_t)(n + 1) * 4, cudaMemcpyHostToDevice, st);
-    cudaMemsetAsync(s.off_fill, 0, (size_t)n * 4, st);
+    cudaMemcpyAsync(s.off_pos, pos.data(), (size_t)(n + 1) * 8, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(s.off_cursor, head, sizeof(head), cudaMemcpyHostToDevice, st);
-    if ((e = cub::DeviceScan::ExclusiveSum(b[9].p, scan_bytes, s.off_cnt, s.off_pos, n + 1, st)) != cudaSuccess)
-        return cuda_fail(ctx, e, "merge check scan");
-    offer_scatter_kernel<<<grid_for(ctx), 256, 0, st>>>(s);
     const size_t mg_smem = (size_t)mg_warps * s.mg_warp_bytes;
     if (mg_smem > 48 * 1024 &&
         (e = cudaFuncSetAttribute(offer_merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mg_smem)) != cudaSuccess)
@@ -1622,6 +1669,13 @@ extern "C" int kg_join_merge_check(kg_ctx *ctx, unsigned n, unsigned L, unsigned
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(ctx, e, "merge check");
     for (size_t x = 0; x < n; ++x)
         for (uint32_t j = 0; j < s.Lp; ++j) { pool_d[x * s.Lp + j] = hd[x * s.PS + j]; pool_i[x * s.Lp + j] = hi[x * s.PS + j]; }
+    return KG_OK;
+}
+
+extern "C" int kg_set_join_offer_capacity(kg_ctx *ctx, size_t offers) {
+    if (!ctx) return KG_E_INVALID;
+    std::lock_guard<std::mutex> guard(ctx->mu);
+    ctx->offer_cap = offers;
     return KG_OK;
 }
 

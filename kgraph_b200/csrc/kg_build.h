@@ -47,6 +47,8 @@ struct BuildState {
     uint64_t *off_pos;
     uint32_t mg_warp_bytes;              // shared memory per merging warp
     uint32_t jt_rows;                    // rows the shared-memory join stages per node (0: join_kernel)
+    uint32_t node_lo, node_hi;           // the join's nodes in this round (deferred joins go in rounds
+                                         // whose offers fit the record buffer)
 };
 // Source-node word of a deferred offer: set when the offer is the pair's
 // x <- y insert, whose position decides the source node's `found`.

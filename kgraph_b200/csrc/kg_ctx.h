@@ -94,6 +94,7 @@ struct kg_ctx {
     kgb::DevBuf joinq, joinaux, joinb;   // tensor-core join: candidate queue, worst-case prefix, round bounds
     kgb::DevBuf offer_lin, offer_grp, offer_aux, offer_scan;   // deferred join inserts (kg_build.cu)
     int join_inserts = KG_INSERTS_AUTO;
+    size_t offer_cap = 0;             // record-buffer capacity of deferred inserts, in offers (0: automatic)
     bool join_tile = true;            // FP32 join with each node's lists staged in shared memory
     kg_join_stats last_join{};
     // tensor-core brute force (kg_bruteforce.cu): BF16 centred rows, row terms, mean + extents, work space

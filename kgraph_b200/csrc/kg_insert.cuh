@@ -101,4 +101,60 @@ __device__ __forceinline__ uint32_t locked_insert(const BuildState &s, uint32_t 
     return r;
 }
 
+// One pass of 8 pairs (one per 4-lane group: lanes 4p..4p+3 hold pair p's
+// x, y and distance, valid marking a pair to evaluate, n the node whose join
+// made it): the unlocked radius pre-test for both directions
+// (kgraph.cpp:725), then Nhood::parallel_try_insert of the offers that passed
+// -- recorded for the deferred merge while the record buffer has room, else
+// under the target's lock here.  A locked x <- y insert that lands below K
+// (kgraph.cpp:808-810) sets uu, or with set_found the found flag of its pair's
+// node directly; comps counts the pairs (the reference's cc).
+__device__ __forceinline__ void settle_pass(const BuildState &s, int lane, int t, bool valid, uint32_t x, uint32_t y,
+                                            float dd, uint32_t n, unsigned long long &comps, bool &uu,
+                                            InsertTally &tally, bool set_found = false) {
+    const float rx = (valid && t == 0) ? *reinterpret_cast<volatile float *>(s.radius + x) : 0.f;
+    const float ry = (valid && t == 1) ? *reinterpret_cast<volatile float *>(s.radius + y) : 0.f;
+    const unsigned vm_all = __ballot_sync(FULL, valid && t == 0);
+    unsigned nx = __ballot_sync(FULL, valid && t == 0 && !(dd > rx));
+    unsigned ny = __ballot_sync(FULL, valid && t == 1 && !(dd > ry));
+    comps += __popc(vm_all);
+    if (s.off_lin && (nx | ny)) {
+        // deferred: the offers go to the grouped merge after the join (one
+        // cursor atomic per pass); those beyond the buffer's capacity are
+        // inserted here under the lock
+        const unsigned om = nx | ny;
+        unsigned long long b0 = 0;
+        if (lane == 0) b0 = atomicAdd(s.off_cursor, (unsigned long long)__popc(om));
+        b0 = __shfl_sync(FULL, b0, 0);
+        const unsigned long long fit = b0 >= s.off_cap ? 0ull : s.off_cap - b0;
+        const uint32_t rank = __popc(om & ((1u << lane) - 1u));
+        const bool mine = ((om >> lane) & 1u) && rank < fit;
+        if (mine) {
+            const uint32_t tg = t == 0 ? x : y;
+            s.off_lin[b0 + rank] = make_uint4(tg, t == 0 ? y : x, __float_as_uint(dd), n | (t == 0 ? OFFER_UU : 0u));
+            atomicAdd(s.off_cnt + tg, 1u);
+        }
+        const unsigned dm = __ballot_sync(FULL, mine);
+        nx &= ~dm;
+        ny &= ~dm;
+    }
+    // only the pairs with an offer that passed a radius test: a pair both endpoints reject
+    // inserts nothing and leaves r at pool.size() (>= K)
+    unsigned vm = nx | (ny >> 1);
+    while (vm) {
+        const int src = __ffs(vm) - 1;
+        vm &= vm - 1;
+        const uint32_t xg = __shfl_sync(FULL, x, src), yg = __shfl_sync(FULL, y, src);
+        const float dg = __shfl_sync(FULL, dd, src);
+        const uint32_t ng = __shfl_sync(FULL, n, src);
+        uint32_t r = s.Lp;
+        if (nx & (1u << src)) r = locked_insert(s, xg, yg, dg, lane, tally);
+        if (r < s.K) {
+            if (!set_found) uu = true;
+            else if (lane == 0) s.found[ng] = 1u;
+        }
+        if (ny & (1u << (src + 1))) locked_insert(s, yg, xg, dg, lane, tally);
+    }
+}
+
 }  // namespace kgb

@@ -568,22 +568,10 @@ __global__ void __launch_bounds__(256) join_insert_kernel(BuildState s, JoinQueu
         const bool valid = e < end;
         const uint32_t x = valid ? jq.x[e] : 0u, y = valid ? jq.y[e] : 0u, nn = valid ? jq.n[e] : 0u;
         const float dd = pair_dist(s.D, x, y, t, FULL);
-        const float rx = (valid && t == 0) ? *reinterpret_cast<volatile float *>(s.radius + x) : 0.f;
-        const float ry = (valid && t == 1) ? *reinterpret_cast<volatile float *>(s.radius + y) : 0.f;
-        const unsigned nx = __ballot_sync(FULL, valid && t == 0 && !(dd > rx));
-        const unsigned ny = __ballot_sync(FULL, valid && t == 1 && !(dd > ry));
-        unsigned vm = nx | (ny >> 1);   // pairs with an offer that passed a radius test
-        while (vm) {
-            const int src = __ffs(vm) - 1;
-            vm &= vm - 1;
-            const uint32_t xg = __shfl_sync(FULL, x, src), yg = __shfl_sync(FULL, y, src);
-            const uint32_t ng = __shfl_sync(FULL, nn, src);
-            const float dg = __shfl_sync(FULL, dd, src);
-            uint32_t r = s.Lp;
-            if (nx & (1u << src)) r = locked_insert(s, xg, yg, dg, lane, tally);
-            if (r < s.K && lane == 0) s.found[ng] = 1u;
-            if (ny & (1u << (src + 1))) locked_insert(s, yg, xg, dg, lane, tally);
-        }
+        // deferred (the offers to the grouped merge) or locked inserts; the pairs were counted by the filter
+        unsigned long long comps = 0;
+        bool uu = false;
+        settle_pass(s, lane, t, valid, x, y, dd, nn, comps, uu, tally, true);
     }
     if (lane == 0 && tally.attempts) {
         atomicAdd(s.inserts, (unsigned long long)tally.attempts);

@@ -90,9 +90,12 @@ def _serial(case, L, K):
             continue
         key = (_ord(ds[sel]) << np.uint64(32)) | cd[sel].astype(np.uint64)
         sel = sel[np.argsort(key, kind="stable")]
-        d2, i2, l2, r2, r = ko.serial_inserts(pool_d[x], pool_i[x], nodeL[x], radius[x], cd[sel], ds[sel])
+        d2, i2, l2, r2, _ = ko.serial_inserts(pool_d[x], pool_i[x], nodeL[x], radius[x], cd[sel], ds[sel])
         out_d[x], out_i[x], out_L[x], out_r[x] = d2, i2, l2, r2
-        for k, rk in zip(sel, r):
+        # `found` as the same inserts set it in the order the offers arrive (the input order)
+        arr = np.nonzero(tg == x)[0]
+        _, _, _, _, r = ko.serial_inserts(pool_d[x], pool_i[x], nodeL[x], radius[x], cd[arr], ds[arr])
+        for k, rk in zip(arr, r):
             if (sr[k] & UU) and rk < K:
                 found[int(sr[k]) & 0x7FFFFFFF] = 1
     return out_d, out_i, out_L, out_r, found
@@ -126,6 +129,41 @@ def test_merge_in_passes_keeps_the_top_list(gpu_ctx):
         assert len(np.unique(ids)) == Lc
         if Lc == L and rd[x] != FMAX:
             assert rd[x] == pd[x, L - 1]
+
+
+def _graph_recall10(ctx, X):
+    off, ids, dists, M = ctx.graph()
+    samp = np.random.default_rng(3).choice(len(X), 400, replace=False)
+    hit = 0
+    for v in samp:
+        a, b = int(off[v]), int(off[v + 1])
+        row = ids[a:b][np.argsort(dists[a:b], kind="stable")][:10]
+        d = ((X - X[v]) ** 2).sum(1)
+        d[v] = np.inf
+        kth = np.partition(d, 9)[9]
+        hit += int((((X[row] - X[v]) ** 2).sum(1) <= kth).sum())
+    return hit / (400 * 10)
+
+
+def test_deferred_join_in_rounds_and_overflow(gpu_ctx):
+    """A record buffer far smaller than one join's offers: the join runs in
+    64 rounds of consecutive nodes, and offers beyond the buffer within a round
+    take the locked path; the graph keeps the same quality as with the
+    automatic buffer (both are serial orders of the same inserts)."""
+    from kgraph_b200 import capi
+    rng = np.random.default_rng(12)
+    c = rng.uniform(0, 128, (16, 24))
+    X = np.round(np.maximum(c[rng.integers(0, 16, 20000)] + rng.normal(0, 20, (20000, 24)), 0)).astype(np.float32)
+    out = {}
+    for cap in (0, 20000):
+        ctx = capi.Context(0)
+        ctx.set_data(X, "euclidean")
+        ctx.set_join_offer_capacity(cap)
+        ctx.build(K=20, L=40, S=10, R=100, reverse=-1)
+        out[cap] = _graph_recall10(ctx, X)
+        ctx.close()
+    assert out[0] > 0.95
+    assert abs(out[0] - out[20000]) <= 0.005, out
 
 
 def test_deferred_and_locked_builds_agree(gpu_ctx):
