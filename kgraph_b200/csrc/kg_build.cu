@@ -1405,12 +1405,14 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
             if ((e = ctx->joinb.reserve((size_t)(R + 1) * 4)) != cudaSuccess) return cuda_fail(ctx, e, "alloc");
             jq.bounds = ctx->joinb.as<uint32_t>();
             if ((e = join_tc_bounds(st, jpre, N, slab, R, jq.bounds)) != cudaSuccess) return cuda_fail(ctx, e, "join");
-            for (uint32_t r = 0; r < R; ++r) {
-                if (s.off_lin) rec_offers_begin();
+            // the rounds' offers (the queue bounds a round's pairs, not its offers) wait for one
+            // merge after the last round: all of the iteration's inserts after its pairs, a serial
+            // order the reference's threads can take
+            if (s.off_lin) rec_offers_begin();
+            for (uint32_t r = 0; r < R; ++r)
                 if ((e = launch_join_tc(ctx->num_sms, grid_for(ctx), st, s, jq, r, fp8 ? 1 : 0)) != cudaSuccess)
                     return cuda_fail(ctx, e, "join");
-                if (s.off_lin && (e = rec_offers_end(s)) != cudaSuccess) return cuda_fail(ctx, e, "join merge");
-            }
+            if (s.off_lin && (e = rec_offers_end(s)) != cudaSuccess) return cuda_fail(ctx, e, "join merge");
             if ((e = run_graph(g_stats, rec_stats)) != cudaSuccess) return cuda_fail(ctx, e, "statistics graph");
         } else if (pending_update) {
             e = run_graph(g_steady, [&]() -> cudaError_t {
