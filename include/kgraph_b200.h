@@ -116,8 +116,10 @@ int kg_search_batch(kg_ctx *ctx, const float *queries, size_t nq, size_t q_strid
  *   prefetch         neighbour batches whose rows are prefetched into L2 ahead
  *                    of the walk (0 or 2)
  *   regs             registers per thread the kernel is compiled for: 64
- *                    (0 = 64), or 80 (FP32 walk only: fewer spills where
- *                    large pools limit residency anyway)
+ *                    (0 = 64), 80 (FP32 walk only: fewer spills where
+ *                    large pools limit residency anyway) or 56 (the FP32
+ *                    walk with compact entries, blocks of at most 4 warps:
+ *                    36 resident warps per SM instead of 32)
  *   compact          1: 8-byte pool entries instead of 12 (the id in the
  *                    bits N needs, the expansion progress in batches of S in
  *                    the rest of 31 bits; M read again when an entry is

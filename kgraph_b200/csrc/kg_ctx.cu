@@ -593,7 +593,7 @@ int kg_set_search_tuning(kg_ctx *ctx, const kg_search_tuning *t) {
     const SearchShape sh = shape_of(*t);
     if (!search_shape_valid(sh) || sh.split == 0)
         return set_error(ctx, KG_E_INVALID, "search tuning: split must be 2, 4 or 8, warps_per_block 0, 1, 2, 4 or "
-                                            "8, prefetch 0 or 2, regs 0, 64 or 80, compact 0 or 1");
+                                            "8, prefetch 0 or 2, regs 0, 56, 64 or 80, compact 0 or 1");
     ctx->search_shape = sh;
     return KG_OK;
 }
@@ -673,7 +673,7 @@ int kg_search_autotune(kg_ctx *ctx, const float *queries, size_t nq, size_t q_st
     ++variants;
     // the 80-register budget only has FP32-walk variants
     const std::vector<uint32_t> budgets =
-        ctx->search_prec == KG_SEARCH_FP32 ? std::vector<uint32_t>{64u, 80u} : std::vector<uint32_t>{64u};
+        ctx->search_prec == KG_SEARCH_FP32 ? std::vector<uint32_t>{56u, 64u, 80u} : std::vector<uint32_t>{64u};
     // the compact pool entry only where the FP32 walk can use it on this graph
     const uint32_t N = ctx->has_graph ? ctx->gn : ctx->n;
     bool cp_ok = ctx->search_prec == KG_SEARCH_FP32 && ctx->has_graph;

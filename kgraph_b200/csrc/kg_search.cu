@@ -307,11 +307,12 @@ __device__ __forceinline__ void prefetch_crow(const SearchArgs &a, uint32_t id) 
 // compressed rows (1 BF16, 2 FP8) that filter candidates once the pool is full.
 // MB: resident blocks of 256 threads per SM the register allocation is sized
 // for (4: 64 registers per thread; 3: 80, fewer spills for large pools, whose
-// shared memory limits residency anyway).  CP: the compact 8-byte pool entry
+// shared memory limits residency anyway), or 9: blocks of at most 128
+// threads at 56 registers (36 warps per SM instead of 32).  CP: the compact 8-byte pool entry
 // (the host selects it only when every node's expansion fits the progress
 // field: a.cp_idbits id bits, 31 - a.cp_idbits progress bits).
 template <int G, int PF, int PREC, int MB, int CP>
-__global__ void __launch_bounds__(256, MB) search_kernel(SearchArgs a) {
+__global__ void __launch_bounds__(MB == 9 ? 128 : 256, MB) search_kernel(SearchArgs a) {
     extern __shared__ __align__(16) char smem[];
     const uint32_t IDM = CP ? (1u << a.cp_idbits) - 1u : ID_MASK;   // the id bits of a pool word
     const uint32_t PMASK = CP ? ID_MASK >> a.cp_idbits : 0u;        // the progress bits, shifted down
@@ -741,7 +742,10 @@ SearchFn search_fn(uint32_t split, uint32_t prefetch, uint32_t prec, uint32_t re
     const bool pf = prefetch > 0;
     if (prec == 1) return search_fn_prec<1, 4, 0>(split, pf);
     if (prec == 2) return search_fn_prec<2, 4, 0>(split, pf);
-    if (compact) return regs == 80 ? search_fn_prec<0, 3, 1>(split, pf) : search_fn_prec<0, 4, 1>(split, pf);
+    if (compact) {
+        if (regs == 56) return search_fn_prec<0, 9, 1>(split, pf);
+        return regs == 80 ? search_fn_prec<0, 3, 1>(split, pf) : search_fn_prec<0, 4, 1>(split, pf);
+    }
     return regs == 80 ? search_fn_prec<0, 3, 0>(split, pf) : search_fn_prec<0, 4, 0>(split, pf);
 }
 // The compact pool runs where the shape asks for it and the graph allows it.
@@ -750,7 +754,8 @@ bool use_compact(const SearchArgs &a, const SearchShape &sh) { return search_use
 // Warps per block: the requested query tile, or as many as fit 200 KB of
 // shared memory (at most 8); halved until the block fits.
 uint32_t pick_wpb(const SearchShape &sh, size_t warp_bytes) {
-    uint32_t wpb = sh.warps_per_block ? std::min<uint32_t>(sh.warps_per_block, 8) : 8;
+    const uint32_t most = sh.regs == 56 ? 4u : 8u;   // the 56-register variant takes blocks of at most 128 threads
+    uint32_t wpb = sh.warps_per_block ? std::min<uint32_t>(sh.warps_per_block, most) : most;
     while (wpb > 1 && (size_t)wpb * warp_bytes > 200 * 1024) wpb >>= 1;
     return wpb;
 }
@@ -766,7 +771,7 @@ bool search_shape_valid(const SearchShape &sh) {
     const bool wpb_ok = sh.warps_per_block == 0 || sh.warps_per_block == 1 || sh.warps_per_block == 2 ||
                         sh.warps_per_block == 4 || sh.warps_per_block == 8;
     const bool pf_ok = sh.prefetch == 0 || sh.prefetch == 2;
-    const bool regs_ok = sh.regs == 0 || sh.regs == 64 || sh.regs == 80;
+    const bool regs_ok = sh.regs == 0 || sh.regs == 56 || sh.regs == 64 || sh.regs == 80;
     return split_ok && wpb_ok && pf_ok && regs_ok && sh.compact <= 1;
 }
 
