@@ -51,8 +51,8 @@ TARGET = 0.95
 # queries, K=10), per launch: the plain walk at P=1000, the router-seeded walk
 # at P=5, and the local join (the shared-memory join, the offers' scatter and
 # the pools' merge) summed over the iterations of one warm build.
-SEARCH_DRAM_BYTES_PER_LAUNCH = 136.02e9
-ROUTER_SEARCH_DRAM_BYTES_PER_LAUNCH = 17.35e9
+SEARCH_DRAM_BYTES_PER_LAUNCH = 136.18e9
+ROUTER_SEARCH_DRAM_BYTES_PER_LAUNCH = 17.53e9
 BUILD_JOIN_DRAM_BYTES = 364.7e9
 
 
@@ -552,6 +552,9 @@ def main():
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the reference's CPU build of the same graph (build parity, ~35 s on 16 threads)")
     ap.add_argument("--router-train", type=int, default=ROUTER_TRAIN)
+    ap.add_argument("--offer-cap", type=int, default=0,
+                    help="bound on the deferred join inserts' record buffers, in offers (0: automatic); keeps the "
+                         "device memory of small profiling runs low")
     ap.add_argument("--join", default=None, choices=["auto", "fp32", "bf16", "bf16_always", "fp8", "fp8_always"],
                     help="local-join precision of a --workload run (default: the workload's own)")
     ap.add_argument("--workload", default="c2", choices=["c2"] + sorted(WORKLOADS),
@@ -577,6 +580,8 @@ def main():
     ctx = capi.Context(local)
     capi.set_verbosity(0)
     ctx.set_data(X, "euclidean")
+    if args.offer_cap:
+        ctx.set_join_offer_capacity(args.offer_cap)
     # build (timed on the device by the library's own CUDA events): the first
     # build of a process also pays one-time costs (module loading, state
     # allocation, graph capture), so it is reported apart from the warm ones
