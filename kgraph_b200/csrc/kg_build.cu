@@ -420,10 +420,47 @@ __device__ __forceinline__ uint32_t f2ord(float f) {
 }
 __device__ __forceinline__ float ord2f(uint32_t u) { return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u); }
 
+// Ascending bitonic sort of the 32 E keys at keys[0, 32 E) by one warp, in
+// registers: lane l holds elements l E .. l E + E - 1, so partners closer than
+// E are in the lane and farther ones are an XOR shuffle away.
+template <int E>
+__device__ __forceinline__ void warp_sort_keys(unsigned long long *keys, int lane) {
+    unsigned long long v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = keys[lane * E + e];
+#pragma unroll
+    for (int k = 2; k <= 32 * E; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            if (j >= E) {
+                const int lj = j / E;
+                const bool lower = (lane & lj) == 0;
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const unsigned long long o = __shfl_xor_sync(FULL, v[e], lj);
+                    const bool asc = ((lane * E + e) & k) == 0;
+                    v[e] = (lower == asc) ? (v[e] < o ? v[e] : o) : (v[e] > o ? v[e] : o);
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    if (e & j) continue;
+                    const bool asc = ((lane * E + e) & k) == 0;
+                    const unsigned long long a = v[e], b = v[e | j];
+                    if ((a > b) == asc) { v[e] = b; v[e | j] = a; }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < E; ++e) keys[lane * E + e] = v[e];
+    __syncwarp();
+}
+
 constexpr uint32_t MG_CH = 512;     // offers merged per pass at most (sorted in shared memory)
 constexpr uint32_t MG_PASS = 224;   // offers a value-mode pass aims at
 constexpr int MG_WARPS = 8;
-size_t merge_warp_bytes(uint32_t PS) { return (size_t)MG_CH * 24 + (size_t)PS * 16; }
+size_t merge_warp_bytes(uint32_t PS) { return (size_t)MG_CH * 20 + (size_t)PS * 16; }
 
 // Nhood::parallel_try_insert (kgraph.cpp:723-736) of every deferred offer
 // into its pool, one warp per pool, without locks (the join has finished).
@@ -448,8 +485,7 @@ __global__ void __launch_bounds__(MG_WARPS * 32) offer_merge_kernel(BuildState s
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     unsigned char *wbase = mg_smem + (size_t)wib * s.mg_warp_bytes;
     unsigned long long *keys = reinterpret_cast<unsigned long long *>(wbase);
-    uint32_t *vals = reinterpret_cast<uint32_t *>(keys + MG_CH);
-    uint32_t *paux = vals + MG_CH;                              // p of a non-duplicate, else ~0
+    uint32_t *paux = reinterpret_cast<uint32_t *>(keys + MG_CH);   // p of a non-duplicate, else ~0
     uint32_t *qaux = paux + MG_CH;                              // its index among the non-duplicates
     float *acc_d = reinterpret_cast<float *>(qaux + MG_CH);     // the accepted offers, in order
     float *pdA = acc_d + MG_CH;
@@ -590,10 +626,7 @@ __global__ void __launch_bounds__(MG_WARPS * 32) offer_merge_kernel(BuildState s
                         }
                         const unsigned bal = __ballot_sync(FULL, in);
                         const uint32_t pos = cm + __popc(bal & ((1u << lane) - 1u));
-                        if (in && pos < MG_CH) {
-                            keys[pos] = ((unsigned long long)ko << 32) | o.y;
-                            vals[pos] = o.w;
-                        }
+                        if (in && pos < MG_CH) keys[pos] = ((unsigned long long)ko << 32) | o.y;
                         cm += __popc(bal);
                     }
                     if (cm <= MG_CH) {
@@ -621,10 +654,7 @@ __global__ void __launch_bounds__(MG_WARPS * 32) offer_merge_kernel(BuildState s
                     const unsigned bal = __ballot_sync(FULL, in);
                     const uint32_t take = min((uint32_t)__popc(bal), MG_CH - cm);
                     const uint32_t rank = __popc(bal & ((1u << lane) - 1u));
-                    if (in && rank < take) {
-                        keys[cm + rank] = ((unsigned long long)ko << 32) | o.y;
-                        vals[cm + rank] = o.w;
-                    }
+                    if (in && rank < take) keys[cm + rank] = ((unsigned long long)ko << 32) | o.y;
                     cursor += (take < (uint32_t)__popc(bal)) ? (uint32_t)(__fns(bal, 0, take + 1)) : 32u;
                     cm += take;
                 }
@@ -634,28 +664,14 @@ __global__ void __launch_bounds__(MG_WARPS * 32) offer_merge_kernel(BuildState s
             rem -= cm;
             uint32_t P2 = 32;
             while (P2 < cm) P2 <<= 1;
-            for (uint32_t k = cm + lane; k < P2; k += 32) {
-                keys[k] = ~0ull;
-                vals[k] = 0;
-            }
+            for (uint32_t k = cm + lane; k < P2; k += 32) keys[k] = ~0ull;
             __syncwarp();
-            for (uint32_t kk = 2; kk <= P2; kk <<= 1) {   // bitonic sort, ascending (distance, id)
-                for (uint32_t jj = kk >> 1; jj > 0; jj >>= 1) {
-                    for (uint32_t i = lane; i < P2; i += 32) {
-                        const uint32_t ixj = i ^ jj;
-                        if (ixj > i) {
-                            const unsigned long long a = keys[i], b = keys[ixj];
-                            if ((a > b) == ((i & kk) == 0)) {
-                                keys[i] = b;
-                                keys[ixj] = a;
-                                const uint32_t t = vals[i];
-                                vals[i] = vals[ixj];
-                                vals[ixj] = t;
-                            }
-                        }
-                    }
-                    __syncwarp();
-                }
+            switch (P2) {   // ascending (distance, id)
+                case 32: warp_sort_keys<1>(keys, lane); break;
+                case 64: warp_sort_keys<2>(keys, lane); break;
+                case 128: warp_sort_keys<4>(keys, lane); break;
+                case 256: warp_sort_keys<8>(keys, lane); break;
+                default: warp_sort_keys<16>(keys, lane); break;
             }
             // positions of the non-duplicates
             uint32_t nnd = 0;
