@@ -46,10 +46,10 @@ struct SearchArgs {
 // Launch shape of the search kernel: the D-split (lanes per distance, 2/4/8;
 // 32/split candidates per pass), the query tile (warps = queries per block,
 // 1/2/4/8; 0 = as many as fit, at most 8), the L2 prefetch depth (0 or 2
-// neighbour batches), the register budget per thread (64, or 80 for the
-// FP32 walk; 0 = 64) and the pool entry (compact = 1: 8 bytes instead of 12,
-// FP32 walk only, where SearchArgs::compact_ok).  Every shape computes the
-// same bits.
+// neighbour batches), the register budget per thread (64; 80 for the FP32
+// walk; 56 for the compact FP32 walk in blocks of at most 4 warps; 0 = 64)
+// and the pool entry (compact = 1: 8 bytes instead of 12, FP32 walk only,
+// where SearchArgs::compact_ok).  Every shape computes the same bits.
 struct SearchShape {
     uint32_t split = 4, warps_per_block = 0, prefetch = 2, regs = 64, compact = 1;
 };
