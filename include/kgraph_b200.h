@@ -350,9 +350,12 @@ int kg_set_join_precision(kg_ctx *ctx, int mode);
  *   KG_INSERTS_DEFERRED  the join records every offer that passes the unlocked
  *                        radius test; the offers are then grouped by target and
  *                        each pool takes its own in one merge, in ascending
- *                        (distance, id) order -- a serial order of the same
- *                        inserts that the reference's threads can produce, with
- *                        the same duplicate, radius, L and `found` rules; offers
+ *                        (distance, id) order (inserts into different pools
+ *                        touch disjoint state: a pool's outcome depends only on
+ *                        the order of its own offers, which the reference's
+ *                        threads leave arbitrary), with the same duplicate,
+ *                        radius and L rules, and `found` as the inserts set it
+ *                        in the offers' arrival order; offers
  *                        beyond the record buffer's capacity (sized from free
  *                        device memory, at most 20 GB; a join that needs more
  *                        runs in rounds of consecutive nodes) are inserted under

@@ -464,8 +464,10 @@ size_t merge_warp_bytes(uint32_t PS) { return (size_t)MG_CH * 20 + (size_t)PS * 
 
 // Nhood::parallel_try_insert (kgraph.cpp:723-736) of every deferred offer
 // into its pool, one warp per pool, without locks (the join has finished).
-// A pool takes its offers in ascending (distance, id) order -- a serial order
-// the reference's threads can produce -- in passes of up to MG_CH, each pass
+// A pool takes its offers in ascending (distance, id) order -- inserts into
+// different pools touch disjoint state, so a pool's outcome depends only on
+// the order of its own offers, which the reference's threads leave arbitrary
+// -- in passes of up to MG_CH, each pass
 // in one merge that reproduces the successive UpdateKnnListHelper calls
 // (kgraph.cpp:176-202):
 //  * an offer equal to an earlier one or to a pool entry (same id, same
@@ -1310,8 +1312,8 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
     // the statistics with their copies to the host, and the update.
     // A deferred join goes in rounds of consecutive nodes (join, grouping and
     // merge each), as many as keep a round's offers -- at most 2 x C(2S, 2)
-    // per node in the first iteration -- within the record buffer; any order
-    // of rounds is a serial order of the same inserts.
+    // per node in the first iteration -- within the record buffer; each pool
+    // then takes its offers round by round, one more order of its own offers.
     const uint32_t join_rounds =
         s.off_lin ? (uint32_t)std::min<uint64_t>(64, std::max<uint64_t>(1, ((uint64_t)N * 2 * S * (2 * S - 1) + s.off_cap - 1) / s.off_cap))
                   : 1u;
@@ -1422,8 +1424,8 @@ extern "C" int kg_build(kg_ctx *ctx, const kg_index_params *params, kg_index_inf
             jq.bounds = ctx->joinb.as<uint32_t>();
             if ((e = join_tc_bounds(st, jpre, N, slab, R, jq.bounds)) != cudaSuccess) return cuda_fail(ctx, e, "join");
             // the rounds' offers (the queue bounds a round's pairs, not its offers) wait for one
-            // merge after the last round: all of the iteration's inserts after its pairs, a serial
-            // order the reference's threads can take
+            // merge after the last round: each pool takes all of its offers of the iteration
+            // together, in the merge's order
             if (s.off_lin) rec_offers_begin();
             for (uint32_t r = 0; r < R; ++r)
                 if ((e = launch_join_tc(ctx->num_sms, grid_for(ctx), st, s, jq, r, fp8 ? 1 : 0)) != cudaSuccess)

@@ -149,7 +149,8 @@ def test_deferred_join_in_rounds_and_overflow(gpu_ctx):
     """A record buffer far smaller than one join's offers: the join runs in
     64 rounds of consecutive nodes, and offers beyond the buffer within a round
     take the locked path; the graph keeps the same quality as with the
-    automatic buffer (both are serial orders of the same inserts)."""
+    automatic buffer (both give each pool its offers in an order the
+    reference's interleavings allow)."""
     from kgraph_b200 import capi
     rng = np.random.default_rng(12)
     c = rng.uniform(0, 128, (16, 24))
