@@ -53,7 +53,7 @@ TARGET = 0.95
 # the pools' merge) summed over the iterations of one warm build.
 SEARCH_DRAM_BYTES_PER_LAUNCH = 136.18e9
 ROUTER_SEARCH_DRAM_BYTES_PER_LAUNCH = 17.53e9
-BUILD_JOIN_DRAM_BYTES = 364.7e9
+BUILD_JOIN_DRAM_BYTES = 377.8e9
 
 
 def _sample(c, n, rng, d):
@@ -879,8 +879,8 @@ def main():
                                        "unit": "GB/s", "frac": build_bytes / (build_ms / 1000) / 1e9 / hbm,
                                        "peak_source": peak_source, "traffic": BUILD_JOIN_DRAM_BYTES,
                                        "traffic_note": "join_tile_kernel + offer_scatter_kernel + offer_merge_kernel "
-                                                       "launches of one build; each node's rows are read once into "
-                                                       "shared memory",
+                                                       "launches of one build; each node's rows are read once, the "
+                                                       "first 24 KB of them into shared memory, the rest from L2",
                                        "bytes": "join list entries x (4 D + 4) + iterations run x N x 2 (L+1) x 12"}},
                 "build_parity": parity,
                 # per step: the queries in, and the ids buffer in (the library keeps a caller's entries
