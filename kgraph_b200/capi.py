@@ -165,6 +165,18 @@ def _ptr(a):
     return a.ctypes.data_as(C.c_void_p)
 
 
+def _set_fields(p, kw):
+    """Keyword arguments onto a parameter struct; a name that is not one of its
+    fields raises TypeError (ctypes would keep it as a plain attribute and the
+    library would never see it)."""
+    names = {f for f, _ in type(p)._fields_}
+    for k, v in kw.items():
+        if k not in names:
+            raise TypeError("%s has no parameter %r (fields: %s)" % (type(p).__name__, k, ", ".join(sorted(names))))
+        setattr(p, k, v)
+    return p
+
+
 class KGError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(msg)
@@ -213,8 +225,7 @@ class Context:
     def build(self, **kw):
         p = IndexParams()
         self.L.kg_index_params_default(C.byref(p))
-        for k, v in kw.items():
-            setattr(p, k, v)
+        _set_fields(p, kw)
         info = IndexInfo()
         self._check(self.L.kg_build(self.h, C.byref(p), C.byref(info)))
         return {f: getattr(info, f) for f, _ in IndexInfo._fields_}
@@ -270,8 +281,7 @@ class Context:
         Qtrain = np.ascontiguousarray(Qtrain, np.float32)
         p = RouterParams()
         self.L.kg_router_params_default(C.byref(p))
-        for k, v in kw.items():
-            setattr(p, k, v)
+        _set_fields(p, kw)
         info = RouterInfo()
         self._check(self.L.kg_router_train(self.h, C.byref(p), _ptr(Qtrain), Qtrain.shape[0], Qtrain.strides[0],
                                            C.byref(info)))

@@ -58,7 +58,14 @@ def graph_recall(G, ex_d, K):
 CASES = [("uniform", 12000, 16, "euclidean", dict(K=25, L=50, S=10)),
          ("mixture", 12000, 32, "euclidean", dict(K=20, L=40, S=10)),
          ("sphere", 10000, 24, "angular", dict(K=15, L=40, S=8)),
-         ("uniform", 8000, 20, "l2sqr", dict(K=10, L=30, S=8))]
+         ("uniform", 8000, 20, "l2sqr", dict(K=10, L=30, S=8)),
+         # Wide rows: at D = 600 eight rows no longer fit the shared-memory join's 24 KB and it
+         # takes 48 KB; at D = 1500 not even that, and the warp-per-node join reads the rows from
+         # L2.  Both builds run to convergence (recall 1, delta 0): under the default stop rule the
+         # reference's own recall at D = 600 moves by 0.01 with its seed, with the iteration at
+         # which the control sample first reads 0.99.
+         ("mixture", 4000, 600, "euclidean", dict(K=10, L=30, S=10, recall=1.0, delta=0.0)),
+         ("mixture", 3000, 1500, "euclidean", dict(K=10, L=30, S=10, recall=1.0, delta=0.0))]
 
 
 @pytest.mark.parametrize("kind,n,d,metric,bp", CASES)

@@ -64,3 +64,19 @@ def test_context_creation_fails_cleanly_without_gpu():
     from kgraph_b200 import capi
     with pytest.raises(capi.KGError):
         capi.Context(0)
+
+
+def test_parameter_keywords_must_name_fields():
+    """A misspelt build or router keyword raises instead of landing on the
+    ctypes struct as a plain attribute the library never reads."""
+    from kgraph_b200 import capi
+    p = capi._set_fields(capi.IndexParams(), dict(K=12, recall=1.0, delta=0.0))
+    assert (p.K, p.recall, p.delta) == (12, 1.0, 0.0)
+    with pytest.raises(TypeError, match="recal"):
+        capi._set_fields(capi.IndexParams(), dict(recal=1.0))
+    with pytest.raises(TypeError, match="rand_seed"):
+        capi._set_fields(capi.IndexParams(), dict(rand_seed=1))
+    r = capi._set_fields(capi.RouterParams(), dict(clusters=64, epochs=2))
+    assert (r.clusters, r.epochs) == (64, 2)
+    with pytest.raises(TypeError):
+        capi._set_fields(capi.RouterParams(), dict(epoch=2))
