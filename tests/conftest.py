@@ -25,6 +25,8 @@ def load_golden(name):
 
 
 GOLDEN_CASES = ["u16", "mix32", "ang20", "l2sq24"]
+# rows wider than the tensor-core brute force takes (d = 300)
+WIDE_GOLDEN_CASES = ["mix300"]
 
 
 @pytest.fixture(scope="session")

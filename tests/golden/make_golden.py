@@ -11,7 +11,7 @@ thread so the graph is deterministic -- and stores inputs and outputs:
   the C++ driver reports them), plus the brute-force K-NN.
 
 Run where the reference's sources and oracle/_ref are present:
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]     (no case: all of them)
 The fixtures are committed; the tests never run the reference themselves on
 the GPU box.
 """
@@ -52,6 +52,11 @@ CASES = {
     "ang20": dict(n=1500, d=20, nq=64, metric="angular", kind="normal", seed=13,
                   build=dict(K=8, L=24, S=6, reverse=0),
                   searches=[dict(K=8, P=20), dict(K=8, P=20, M=20), dict(K=8, P=40, T=2), dict(K=8, P=16, S=3)]),
+    # wide rows (d = 300, not a multiple of 16: 12 tail terms): wider than the
+    # tensor-core brute force takes, integer-valued with exact ties
+    "mix300": dict(n=1000, d=300, nq=48, metric="euclidean", kind="mixture", seed=15,
+                   build=dict(K=10, L=30, S=8, reverse=-1),
+                   searches=[dict(K=10, P=30), dict(K=10, P=80, S=5), dict(K=5, P=40, T=2)]),
 }
 # C++ MatrixOracle<l2sqr> through the reference's C++ API (search cost, epsilon, init)
 L2CASE = dict(name="l2sq24", n=1500, d=24, nq=64, seed=14, build=dict(K=10, L=30, S=8, reverse=-1),
@@ -154,14 +159,20 @@ def run_l2(spec, tmp):
     print(spec["name"], "E", len(G.ids), "info", info)
 
 
-def main():
+def main(names):
     if not ko.reference_available("v4"):
         raise SystemExit("oracle/_ref/v4 is not built (make -C oracle ref)")
+    known = list(CASES) + [L2CASE["name"]]
+    for n in names:
+        if n not in known:
+            raise SystemExit("unknown case %r (cases: %s)" % (n, ", ".join(known)))
     with tempfile.TemporaryDirectory() as tmp:
         for name, spec in CASES.items():
-            run_case(name, spec, tmp)
-        run_l2(L2CASE, tmp)
+            if not names or name in names:
+                run_case(name, spec, tmp)
+        if not names or L2CASE["name"] in names:
+            run_l2(L2CASE, tmp)
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

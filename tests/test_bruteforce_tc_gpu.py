@@ -10,7 +10,7 @@ reference's own brute-force output in the golden fixtures.
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_CASES, load_golden
+from conftest import GOLDEN_CASES, WIDE_GOLDEN_CASES, load_golden
 
 pytestmark = pytest.mark.gpu
 
@@ -48,6 +48,24 @@ def test_tensor_bruteforce_matches_reference_fixture(name):
         ctx.set_data(g["X"], g["metric"])
         (ids, d, cnt, cost), st = run(ctx, g["Q"], 10, "tensor")
         assert st["tensor"] == 1
+        assert (cnt == 10).all() and (cost == 1.0).all()
+        assert (ids == g["bf_ids"]).all()
+        assert (bits(d) == bits(g["bf_dists"])).all()
+    finally:
+        ctx.close()
+
+
+@pytest.mark.parametrize("name", WIDE_GOLDEN_CASES)
+def test_rows_too_wide_for_the_tiles_take_the_scan(name):
+    """Rows wider than 256 floats: the tensor mode falls back to the warp scan
+    (the tile path stages at most 256 columns), with the reference's results."""
+    from kgraph_b200 import capi
+    g = load_golden(name)
+    ctx = capi.Context(0)
+    try:
+        ctx.set_data(g["X"], g["metric"])
+        (ids, d, cnt, cost), st = run(ctx, g["Q"], 10, "tensor")
+        assert st["tensor"] == 0
         assert (cnt == 10).all() and (cost == 1.0).all()
         assert (ids == g["bf_ids"]).all()
         assert (bits(d) == bits(g["bf_dists"])).all()

@@ -9,7 +9,7 @@ fresh random inputs.
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_CASES, load_golden
+from conftest import GOLDEN_CASES, WIDE_GOLDEN_CASES, load_golden
 from oracle import kgoracle as ko
 
 
@@ -17,7 +17,7 @@ def bits(a):
     return np.ascontiguousarray(a, np.float32).view(np.uint32)
 
 
-@pytest.mark.parametrize("name", GOLDEN_CASES)
+@pytest.mark.parametrize("name", GOLDEN_CASES + WIDE_GOLDEN_CASES)
 def test_oracle_search_matches_reference_fixtures(name):
     g = load_golden(name)
     G = ko.read_index(g["index_bytes"])
@@ -37,7 +37,7 @@ def test_oracle_search_matches_reference_fixtures(name):
             assert (bits(d) == bits(g["s%d_dists" % i])).all(), (name, s)
 
 
-@pytest.mark.parametrize("name", GOLDEN_CASES)
+@pytest.mark.parametrize("name", GOLDEN_CASES + WIDE_GOLDEN_CASES)
 def test_oracle_bruteforce_matches_reference_fixtures(name):
     g = load_golden(name)
     o = ko.Oracle(g["X"], g["metric"])
@@ -46,7 +46,7 @@ def test_oracle_bruteforce_matches_reference_fixtures(name):
     assert (bits(d) == bits(g["bf_dists"])).all()
 
 
-@pytest.mark.parametrize("name", GOLDEN_CASES)
+@pytest.mark.parametrize("name", GOLDEN_CASES + WIDE_GOLDEN_CASES)
 def test_oracle_single_thread_build_is_the_reference_graph(name):
     g = load_golden(name)
     ref = ko.read_index(g["index_bytes"])

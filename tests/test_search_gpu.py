@@ -8,7 +8,7 @@ batches, T > 1, init seeds, epsilon and the P >= N brute-force path.
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_CASES, load_golden
+from conftest import GOLDEN_CASES, WIDE_GOLDEN_CASES, load_golden
 from oracle import kgoracle as ko
 
 pytestmark = pytest.mark.gpu
@@ -26,7 +26,7 @@ def assert_rows_equal(ids, d, cnt, rids, rd, rcnt):
         assert (bits(d[q, :c]) == bits(rd[q, :c])).all(), q
 
 
-@pytest.mark.parametrize("name", GOLDEN_CASES)
+@pytest.mark.parametrize("name", GOLDEN_CASES + WIDE_GOLDEN_CASES)
 def test_search_matches_reference_fixtures(gpu_ctx, name):
     g = load_golden(name)
     G = ko.read_index(g["index_bytes"])
@@ -49,7 +49,7 @@ def test_search_matches_reference_fixtures(gpu_ctx, name):
             assert (bits(d) == bits(g["s%d_dists" % i])).all()
 
 
-@pytest.mark.parametrize("name", GOLDEN_CASES)
+@pytest.mark.parametrize("name", GOLDEN_CASES + WIDE_GOLDEN_CASES)
 def test_bruteforce_matches_reference_fixtures(name):
     from kgraph_b200 import capi
     g = load_golden(name)
