@@ -152,3 +152,26 @@ def test_python_module_load_search_save_roundtrip(tmp_path):
     assert (bits(a.dists) == bits(b.dists)).all()
     bf = kgraph.KGraph(g["X"], "euclidean").search(g["Q"], K=10, withDistance=True)
     assert (bf[0] == g["bf_ids"]).all()
+
+
+def test_empty_query_batch(gpu_ctx, tmp_path):
+    """A batch of zero queries returns empty results and launches nothing,
+    through the C-ABI and the Python module (python-api.cpp:266-273 sizes the
+    result from the query count: 0 x K)."""
+    import kgraph_b200 as kgraph
+    g = load_golden("u16")
+    G = ko.read_index(g["index_bytes"])
+    gpu_ctx.set_data(g["X"], g["metric"])
+    gpu_ctx.set_graph(G.offsets, G.ids, G.dists, G.M)
+    Q0 = np.zeros((0, g["X"].shape[1]), np.float32)
+    ids, d, cnt, cost = gpu_ctx.search(Q0, K=10, P=40)
+    assert ids.shape == (0, 10) and d.shape == (0, 10) and cnt.shape == (0,) and cost.shape == (0,)
+    p = tmp_path / "ref.idx"
+    p.write_bytes(g["index_bytes"].tobytes())
+    k = kgraph.KGraph(g["X"], "euclidean")
+    k.load(str(p))
+    r, rd = k.search(Q0, K=10, withDistance=True)
+    assert r.shape == (0, 10) and rd.shape == (0, 10)
+    # and the index still answers a real batch afterwards
+    ids, d, cnt, cost = gpu_ctx.search(g["Q"], **g["searches"][0])
+    assert (ids == g["s0_ids"]).all()
