@@ -865,6 +865,9 @@ def main():
                 "build": {"seconds": build_ms / 1000, "wall_s": build_wall, "info": info,
                           "first_build_seconds": cold_ms / 1000, "first_build_wall_s": cold_wall,
                           "warm_builds_seconds": [b[0] / 1000 for b in builds],
+                          # device ms of each iteration run, per warm build (where a slower build spends it)
+                          "warm_builds_iteration_ms": [[round(r["ms"], 2) for r in b[4] if r["ms"] > 0]
+                                                       for b in builds],
                           "graph_launches": build_graphs,
                           "work": {"join_pairs": b_pairs, "join_list_entries": b_lists, "iterations": b_iters,
                                    "iterations_run": b_run},
