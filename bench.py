@@ -79,7 +79,7 @@ def make_data(n=N_BASE, nq=N_QUERIES, d=DIM, centres=N_CENTRES, seed=1, rank=0, 
 
 
 def exact_topk_fp64(Xt, Qt, K, torch):
-    """Exact K-NN by FP64 GEMM on the GPU (the recall judge; integer data is exact in FP64)."""
+    """Exact K-NN by FP64 GEMM on the GPU (the recall ground truth; integer data is exact in FP64)."""
     xn = (Xt * Xt).sum(1)
     out_d, out_i = [], []
     for a in range(0, Qt.shape[0], 500):

@@ -154,7 +154,7 @@ namespace kgraph {
         }
         virtual void get_nn(unsigned id, unsigned *nns, float *dists, unsigned *M, unsigned *L) const = 0;
         virtual void reverse(int) = 0;
-        /// Extension of this build, no counterpart in the reference: the C-ABI
+        /// Extension of this library, no counterpart in the reference: the C-ABI
         /// context of this index (a kg_ctx *, include/kgraph_b200.h) with the
         /// oracle's dataset bound to it, for the calls the reference's interface
         /// has no place for (learned router, distance filter, search autotuner).

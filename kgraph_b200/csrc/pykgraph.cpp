@@ -99,7 +99,7 @@ public:
         hasIndex = true;
     }
 
-    // ---- extensions of this build (no counterpart in the reference's module)
+    // ---- extensions of this library (no counterpart in the reference's module)
 
     // The index's C-ABI context with this object's dataset bound to it.
     kg_ctx *native() {
@@ -253,7 +253,7 @@ PYBIND11_MODULE(_kgraph, module) {
              py::arg("P") = kgraph::default_P, py::arg("M") = kgraph::default_M, py::arg("S") = kgraph::default_S,
              py::arg("T") = kgraph::default_T, py::arg("threads") = 0, py::arg("withDistance") = false,
              py::arg("blas") = false, py::arg("router") = 0)
-        // extensions of this build
+        // extensions of this library
         .def("train_router", &PyKGraph::train_router, "learned entry router (kg_router_train)", py::arg("queries"),
              py::arg("clusters") = 1024, py::arg("hidden") = 256, py::arg("kmeans_iters") = 8,
              py::arg("label_P") = 1000, py::arg("epochs") = 4, py::arg("batch") = 1024, py::arg("lr") = 2e-3f,

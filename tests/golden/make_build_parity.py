@@ -19,7 +19,7 @@ all three results are kept.  Per build:
                    its fixed seeds) over the 1,000 queries, ties counted.
 
 Exact distances are computed in FP64, which is exact on integer data, so the
-judge does not depend on any FP32 summation order.  The GPU test regenerates
+ground truth does not depend on any FP32 summation order.  The GPU test regenerates
 the same data from the same seeds and compares its graph's figures with these.
 
 Run in the build container (needs oracle/_ref):
@@ -114,7 +114,7 @@ def main():
     json.dump({"data": {"N": N, "D": D, "centres": CENTRES, "queries": NQ, "node_sample": NSAMPLE,
                         "seeds": {"data": 21, "sample": 22, "queries": 23}},
                "build": BUILD, "P": P_LIST, "reference_builds": builds,
-               # the judge's exact 10th-nearest squared distances (integers), stored so the test need not
+               # the ground truth's exact 10th-nearest squared distances (integers), stored so the test need not
                # recompute them
                "node_kth": [int(v) for v in node_kth], "query_kth": [int(v) for v in query_kth]},
               open(OUT, "w"))

@@ -1,6 +1,6 @@
 """bench.py's host-side helpers, without a GPU: the index writer it hands the
 reference's CPU search, the synthetic workload generators, the tie-aware
-recall judge and the roofline peak lookup."""
+recall ground truth and the roofline peak lookup."""
 import os
 import sys
 
@@ -59,7 +59,7 @@ def test_workload_generators(name):
     assert (X2 == X).all()   # seeded
 
 
-def test_recall_judge_is_tie_aware():
+def test_recall_ground_truth_is_tie_aware():
     import torch
     rng = np.random.default_rng(1)
     X = np.round(rng.random((400, 8)) * 3).astype(np.float32)   # many exact ties

@@ -12,7 +12,7 @@ python-api.cpp:378-388) on the same data, within 0.005:
 
 The reference's figures (three builds; its build is nondeterministic under
 OpenMP) are committed in tests/golden/build_parity_mix128.json by
-tests/golden/make_build_parity.py, with the judge's exact FP64 distances.
+tests/golden/make_build_parity.py, with the ground truth's exact FP64 distances.
 """
 import json
 import os

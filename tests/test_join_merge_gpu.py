@@ -6,14 +6,15 @@ merge must leave the pool, its list length L, its radius and the source
 nodes' `found` flags exactly as the reference's Nhood::parallel_try_insert
 (kgraph.cpp:723-736, UpdateKnnListHelper kgraph.cpp:176-202) leaves them when
 the same offers arrive one after another in that order.  The oracle's serial
-restatement (oracle/kgoracle.cpp kgo_serial_inserts) is the judge: results are
+restatement (oracle/kgoracle.cpp kgo_serial_inserts) decides: results are
 compared bit for bit.  It runs the same Nhood::try_insert as the oracle's
 build, whose single-thread graph equals the reference's own bit for bit
-(tests/test_oracle_pin.py), so the judge is pinned to the reference.  Distances are small integers, so ties at every position
-(the insert-after-equals rule), duplicates of pool entries and of other
-offers, the overflow slot, and pools whose list is full while the stored
-radius is still FLT_MAX (the radius is only set by an insert into a full list)
-are all exercised.
+(tests/test_oracle_pin.py), so the check is pinned to the reference.
+Distances are small integers, so ties at every position (the
+insert-after-equals rule), duplicates of pool entries and of other offers,
+the overflow slot, and pools whose list is full while the stored radius is
+still FLT_MAX (the radius is only set by an insert into a full list) are all
+exercised.
 """
 import numpy as np
 import pytest

@@ -145,7 +145,7 @@ def test_python_module_load_search_save_roundtrip(tmp_path):
     k.save(str(out))
     # Same header, node records, ids and distances; the reference leaves each
     # record's flag and padding bytes uninitialised (kgraph.cpp:67-74, 370),
-    # this build writes zeros there.
+    # this library writes zeros there.
     a, b = ko.read_index(str(out)), ko.read_index(g["index_bytes"])
     assert out.read_bytes()[:20] == g["index_bytes"].tobytes()[:20]
     assert (a.offsets == b.offsets).all() and (a.ids == b.ids).all() and (a.M == b.M).all()

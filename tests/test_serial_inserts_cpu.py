@@ -1,5 +1,5 @@
 """The oracle's serial inserts (oracle/kgoracle.cpp kgo_serial_inserts), the
-judge of the GPU merge of deferred join inserts, against a direct Python
+reference point of the GPU merge test, against a direct Python
 restatement of the reference's rules on small pools:
 
 * Nhood::parallel_try_insert (kgraph.cpp:723-736): an offer beyond the stored
